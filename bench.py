@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark of the greedy selection hot path on B200.
+
+Workload (one bench step): a complete forward selection on the seeded
+generator "fwd-64k": holdout, n_train=65,536, n_val=32,768, p=60, k=10,
+15 greedy steps (60+59+...+46 = 795 candidate scorings).  Metric:
+candidate-evaluations per second, one evaluation being one
+(validation row, training row, candidate feature) triple.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:       inputs resident in HBM; each step = snn_run (initial distance
+            matrix + 15 x [score, reduce, select, commit]) timed with CUDA
+            events on the library's stream.  `e2e` repeats it through the
+            public API from pinned host buffers (upload + run + result read).
+reference:  speedynn's own CPU neighbour scan (get_k_nearest_neighbors_cpu,
+            speedynn/lib/cpu.c:212-252, compiled from the reference sources
+            into oracle/_ref) on a bounded sample of the same workload:
+            sampled validation rows x all 65,536 training rows x all 60
+            candidates of the first step, one process per host core.
+
+N > 1 (torchrun): every rank runs its own selection problem (seed offset by
+rank): independent problems, no collective on the data path; value sums all
+ranks' evaluations over the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = "fwd-64k"
+METRIC = "cand-evals/s (n_val*n_train*candidates per second), greedy forward selection"
+UNIT = "cand-evals/s"
+
+
+def workload_desc(k, steps, n_train, n_val, p):
+    return {"workload": f"{WORKLOAD}: forward selection, holdout, n_train={n_train}, n_val={n_val}, p={p}, k={k}, "
+                        f"{steps} greedy steps (seeded synthetic generator)",
+            "n_train": n_train, "n_val": n_val, "p": p, "k": k, "greedy_steps": steps,
+            "l2": "inputs larger than L2 (distance matrix 8.6 GB)"}
+
+
+def cand_evals(n_rows, n_cols, p, steps):
+    return float(n_rows) * n_cols * sum(p - t for t in range(steps))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[2] > 200.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in load for i in range(4) if r[3][i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median([r[0] for r in load])), "sm_max_mhz": float(max(r[1] for r in rows)),
+                "power_w_max": float(max(r[2] for r in rows)), "samples": len(load), "reasons": reasons}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference: speedynn's own neighbour scan over sampled validation rows
+# ---------------------------------------------------------------------------
+_W = {}
+
+
+def _ref_worker_init(npz_path, k):
+    import ctypes
+    from oracle import ref
+    d = np.load(npz_path)
+    _W["Xv"], _W["yv"], _W["Xt"], _W["yt"] = d["Xval"], d["yval"], d["Xtrain"], d["ytrain"]
+    _W["k"] = k
+    _W["lib"] = ref.load()
+    _W["ct"] = ctypes
+
+
+def _ref_worker_run(rows):
+    """Holdout scoring of validation rows ``rows`` with the reference's own
+    get_k_nearest_neighbors_cpu: the rows are placed in front of the training
+    block as fold 0 (num_per_fold = len(rows)), so each scans exactly the
+    training points; then the kNN mean and squared error as cpu.c:140-150."""
+    ct = _W["ct"]
+    L = _W["lib"]
+    Xv, yv, Xt, yt, k = _W["Xv"], _W["yv"], _W["Xt"], _W["yt"], _W["k"]
+    R = len(rows)
+    Xp = np.ascontiguousarray(np.concatenate([Xv[rows], Xt]), np.float32)
+    yp = np.concatenate([yv[rows], yt]).astype(np.float32)
+    n, p = Xp.shape
+    D = np.zeros((R, n), np.float32)  # step 0 of forward selection: empty committed set
+    ib = np.zeros(k, np.int32)
+    db = np.zeros(k, np.float32)
+    ip = ib.ctypes.data_as(ct.POINTER(ct.c_int))
+    dp = db.ctypes.data_as(ct.POINTER(ct.c_float))
+    ct.c_int.in_dll(L, "dim").value = p
+    ct.c_int.in_dll(L, "num_training_patterns").value = n
+    ct.c_int.in_dll(L, "k_max").value = k
+    ct.c_void_p.in_dll(L, "training_patterns").value = Xp.ctypes.data
+    ct.c_void_p.in_dll(L, "current_dist_matrix").value = D.ctypes.data
+    sse = np.zeros(p, np.float64)
+    t0 = time.perf_counter()
+    for c in range(p):
+        for r in range(R):
+            L.get_k_nearest_neighbors_cpu(r, 0, R, ip, dp, c, 1)
+            pred = np.float32(yp[ib].sum(dtype=np.float32) / np.float32(k))
+            sse[c] += float(yp[r] - pred) ** 2
+    el = time.perf_counter() - t0
+    ct.c_void_p.in_dll(L, "current_dist_matrix").value = None
+    ct.c_void_p.in_dll(L, "training_patterns").value = None
+    return el, float(R) * Xt.shape[0] * p
+
+
+class RefCPU:
+    """Process pool timing the reference's CPU scan; one process per core."""
+
+    def __init__(self, split, k, rows_per_proc, procs=None):
+        import multiprocessing as mp
+        self.procs = procs or len(os.sched_getaffinity(0))
+        fd, self.npz = tempfile.mkstemp(suffix=".npz")
+        os.close(fd)
+        np.savez(self.npz, Xval=split.Xval, yval=split.yval, Xtrain=split.Xtrain, ytrain=split.ytrain)
+        self.pool = mp.get_context("spawn").Pool(self.procs, initializer=_ref_worker_init, initargs=(self.npz, k))
+        self.rows = rows_per_proc
+        self.nval = split.Xval.shape[0]
+        self.calls = 0
+
+    def step(self):
+        """One bounded sample: `procs` disjoint row blocks in parallel."""
+        jobs = []
+        for w in range(self.procs):
+            start = ((self.calls * self.procs + w) * self.rows) % max(1, self.nval - self.rows)
+            jobs.append(list(range(start, start + self.rows)))
+        self.calls += 1
+        t0 = time.perf_counter()
+        res = self.pool.map(_ref_worker_run, jobs)
+        wall = time.perf_counter() - t0
+        evals = sum(r[1] for r in res)
+        return evals, wall
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+        os.unlink(self.npz)
+
+
+def ref_available():
+    return os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libspeedynn_ref.so"))
+
+
+def port_cpu_rate(split, k, rows):
+    """Fallback CPU baseline: the oracle restatement (OpenMP, all cores)."""
+    from oracle import oracle
+    prob = oracle.Problem(split.Xtrain, split.ytrain, split.Xval, split.yval)
+    p = split.Xtrain.shape[1]
+    t0 = time.perf_counter()
+    oracle.step(prob, [k], [], list(range(p)), rows=list(range(rows)), want_neighbours=False)
+    el = time.perf_counter() - t0
+    return float(rows) * split.Xtrain.shape[0] * p / el, el
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    from speedynn_b200 import datagen
+    if rank != 0:
+        return 0
+    split, k, steps = datagen.workload(WORKLOAD)
+    n_train, n_val, p = split.Xtrain.shape[0], split.Xval.shape[0], split.Xtrain.shape[1]
+    cfg = workload_desc(k, steps, n_train, n_val, p)
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg}
+    if ref_available():
+        rc = RefCPU(split, k, args.ref_rows)
+        for _ in range(args.warmup):
+            rc.step()
+        tot_e, tot_t = 0.0, 0.0
+        for _ in range(args.steps):
+            e, t = rc.step()
+            tot_e += e
+            tot_t += t
+        rc.close()
+        v = tot_e / tot_t
+        kind = "reference"
+        sample = (f"speedynn get_k_nearest_neighbors_cpu + kNN mean, {rc.procs} processes x {args.ref_rows} "
+                  f"validation rows x {n_train} training rows x {p} candidates (first greedy step) per bench step")
+        cores = rc.procs
+    else:
+        v, el = port_cpu_rate(split, k, args.ref_rows)
+        kind = "port"
+        cores = len(os.sched_getaffinity(0))
+        sample = f"oracle restatement, {args.ref_rows} validation rows x {n_train} x {p} candidates"
+        tot_t = el * args.steps
+    line.update({"value": v, "ms_per_step": 1000.0 * cand_evals(n_val, n_train, p, steps) / v,
+                 "ms_per_step_note": "extrapolated: full 15-step selection at the measured CPU rate",
+                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "gpu_launches": 0})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from speedynn_b200 import datagen
+    from speedynn_b200.selector import Selector
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = dict(datagen.WORKLOADS[WORKLOAD])
+    k, steps = w.pop("k"), w.pop("select")
+    w["seed"] = w["seed"] + 1000 * rank
+    split = datagen.generate(**w)
+    n_train, n_val, p = split.Xtrain.shape[0], split.Xval.shape[0], split.Xtrain.shape[1]
+    evals = cand_evals(n_val, n_train, p, steps)
+
+    sel = Selector(split.Xtrain, split.ytrain, split.Xval, split.yval, k_vals=[k], num_features=steps,
+                   method="forward", device=local)
+    for _ in range(args.warmup):
+        sel.run()
+
+    gpu_index = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local < len(ids):
+            gpu_index = ids[local]
+    clk = Clocks(gpu_index)
+    barrier()
+    clk.start()
+    tot_ms = score_ms = commit_ms = 0.0
+    score_n = commit_n = launches = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sel.run()
+        tm = sel.timing()
+        tot_ms += tm["total_ms"]
+        score_ms += tm["score_ms"]
+        score_n += tm["score_launches"]
+        commit_ms += tm["commit_ms"]
+        commit_n += tm["commit_launches"]
+        launches += tm["launches"]
+    barrier()
+    wall = time.perf_counter() - t0
+    clocks = clk.stop()
+    res = sel.results()
+    ms_step = allmax(tot_ms / args.steps)
+
+    # end to end through the public API: pinned host inputs uploaded every step, results read back
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t.numpy()
+    hx, hy, hxv, hyv = pinned(split.Xtrain), pinned(split.ytrain), pinned(split.Xval), pinned(split.yval)
+    h2d = hx.nbytes + hy.nbytes + hxv.nbytes + hyv.nbytes
+    from speedynn_b200 import _lib
+    from speedynn_b200._lib import _f32p, ptr
+    L = _lib.lib()
+    barrier()
+    e0 = time.perf_counter()
+    d2h = 0
+    for _ in range(args.steps):
+        _lib.check(L.snn_load(sel._h, ptr(hx, _f32p), ptr(hy, _f32p), ptr(hxv, _f32p), ptr(hyv, _f32p)))
+        _lib.check(L.snn_run(sel._h))
+        r = sel.results()
+        d2h = sum(v.nbytes for v in r.values() if isinstance(v, np.ndarray)) + 8
+    barrier()
+    e2e_s = allmax((time.perf_counter() - e0) / args.steps)
+    sel.close()
+
+    # roofline of the scoring kernel: FP32 pipe (3 rounded ops per evaluation) vs one D read
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    sm = torch.cuda.get_device_properties(local).multi_processor_count
+    mhz = clocks.get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = sm * 128 * mhz * 1e6 * 1e-12  # T ops/s of the FP32 pipe at the sampled clock
+    avg_score_s = score_ms / max(1, score_n) / 1000.0
+    evals_per_launch = evals / steps
+    achieved_fp32 = 3.0 * evals_per_launch / avg_score_s * 1e-12
+    bytes_per_launch = 4.0 * n_val * n_train
+    achieved_hbm = bytes_per_launch / avg_score_s * 1e-9
+
+    line = {"metric": METRIC, "value": world * evals / (ms_step / 1000.0), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload_desc(k, steps, n_train, n_val, p), parallelism=f"independent problems x{world}"),
+            "greedy_step_ms": ms_step / steps,
+            "breakdown_ms_per_step": {"score": score_ms / args.steps, "commit": commit_ms / args.steps,
+                                      "other": (tot_ms - score_ms - commit_ms) / args.steps},
+            "wall_ms_per_step": 1000.0 * wall / args.steps,
+            "e2e": {"value": world * evals / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp32", "kernel": "k_score", "achieved": achieved_fp32, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved_fp32 / fp32_peak,
+                         "peak_source": f"{sm} SMs x 128 FP32 lanes x {mhz:.0f} MHz (sampled median; no FP32 "
+                                        "figure in MEASURED_PEAKS.json); work = 3 rounded FP32 ops per evaluation",
+                         "hbm_achieved_gbs": achieved_hbm, "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src,
+                         "hbm_frac": achieved_hbm / hbm, "traffic": args.traffic},
+            "clocks": clocks,
+            "result": {"ordering": [int(x) for x in res["ordering"][:steps]],
+                       "errors": [float(x) for x in res["errors"][:steps]]}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if ref_available():
+            rc = RefCPU(split, k, args.cpu_rows)
+            e, t = rc.step()
+            rc.close()
+            line["cpu_baseline"] = {"value": e / t, "unit": UNIT, "cores": rc.procs, "kind": "reference",
+                                    "sample": f"speedynn get_k_nearest_neighbors_cpu, {rc.procs} processes x "
+                                              f"{args.cpu_rows} validation rows x {n_train} x {p} candidates"}
+        else:
+            v, el = port_cpu_rate(split, k, args.cpu_rows)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": len(os.sched_getaffinity(0)), "kind": "port",
+                                    "sample": f"oracle restatement, {args.cpu_rows} rows x {n_train} x {p}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-rows", type=int, default=64, help="validation rows per process per reference step")
+    ap.add_argument("--cpu-rows", type=int, default=96, help="validation rows per process for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu dram bytes per scoring launch, scaled to this workload (reported as roofline.traffic)")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,170 @@
+/*
+ * speedynn_b200.h -- C ABI of libspeedynn_b200.so: greedy nearest-neighbour
+ * wrapper feature selection (forward selection / backward elimination scored
+ * by kNN-regression RMSE) on one NVIDIA B200 (sm_100a).
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the names and argument lists of speedynn's
+ *     SWIG-wrapped C API (speedynn/lib/nearest_neighbors_feature_selection.h:59-80,
+ *     typemaps speedynn/lib/nearest_neighbors_feature_selection_float_gpu.i:14-22).
+ *     Like the reference they keep the last result in library state that the
+ *     get_* functions read; unlike it they never exit the process: failures
+ *     return a negative status and set snn_last_error().
+ *
+ *  2. A handle API (snn_*) that adds a train/validation holdout mode, device
+ *     selection, step-wise execution, FP64 errors beside the reference's FP32
+ *     errors, neighbour-list introspection and kernel timing.
+ *
+ * All arrays are plain host pointers owned by the caller, float32 row-major
+ * for matrices ([n][p]), int32 for indices.  No call retains a caller pointer
+ * after it returns.  Calls on one handle must come from one thread at a time;
+ * different handles are independent.  The drop-in layer shares one library
+ * state and is not re-entrant (as in the reference).
+ */
+#ifndef SPEEDYNN_B200_H
+#define SPEEDYNN_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SNN_API __attribute__((visibility("default")))
+#else
+#define SNN_API
+#endif
+
+/* status codes (>= 0 success) */
+#define SNN_OK 0
+#define SNN_ERR_ARG (-1)          /* invalid argument or shape */
+#define SNN_ERR_CUDA (-2)         /* CUDA runtime error, or no usable sm_100 device */
+#define SNN_ERR_NOMEM (-3)        /* device or host allocation failed */
+#define SNN_ERR_UNSUPPORTED (-4)  /* a reference option outside this library's path */
+#define SNN_ERR_NO_WINNER (-5)    /* no candidate had an error below FLT_MAX (e.g. NaN labels) */
+#define SNN_ERR_STATE (-6)        /* call out of order (e.g. run before load) */
+
+/* loss ids, speedynn/base.py:13-23 */
+#define SNN_LOSS_RMSE 0
+
+/* ---------------------------------------------------------------------------
+ * 1. Reference-compatible entry points
+ * ------------------------------------------------------------------------- */
+
+/* Replaces train_forward_selection
+ * (speedynn/lib/nearest_neighbors_feature_selection.h:65, .c:60-65).
+ * CV mode over Xtrain [nXtrain][dXtrain]: folds are contiguous row blocks of
+ * nXtrain / kfold rows (a remainder forms an extra fold).  Returns the final
+ * number of features, or a negative status.  loss_functions[0] must be
+ * SNN_LOSS_RMSE; model_type must be 0 (regression). */
+SNN_API int train_forward_selection(float *Xtrain, int nXtrain, int dXtrain, float *Ytrain, int nYtrain,
+                                    int *kvals, int num_kvals, int num_features, int kfold,
+                                    int *loss_functions, int num_loss_functions, int auto_feature,
+                                    int model_type);
+
+/* Replaces train_backward_selection
+ * (speedynn/lib/nearest_neighbors_feature_selection.h:59, .c:49-54). */
+SNN_API int train_backward_selection(float *Xtrain, int nXtrain, int dXtrain, float *Ytrain, int nYtrain,
+                                     int *kvals, int num_kvals, int num_features, int kfold,
+                                     int *loss_functions, int num_loss_functions, int auto_feature,
+                                     int model_type);
+
+/* Replace the getters of speedynn/lib/nearest_neighbors_feature_selection.h:73-77
+ * (.c:401-432): copy min(n, p) entries (errors: min(n, num_losses*p)) of the
+ * last run's 0/1 mask, ordering and per-step errors (index l*p + i). */
+SNN_API void get_selected_dimensions(int *selected_dimensions_extern, int num_selected_dimensions_extern);
+SNN_API void get_selected_ordering(int *selected_ordering_extern, int num_selected_ordering_extern);
+SNN_API void get_selected_errors(float *selected_errors_extern, int num_selected_errors_extern);
+/* best k of the last winner (nearest_neighbors_feature_selection.c:170, :332) */
+SNN_API int get_final_optimal_model_k(void);
+
+/* Replaces get_loss_all (speedynn/lib/nearest_neighbors_feature_selection.h:78,
+ * loss_functions.c:6-38): a host-side utility over two label vectors, all nine
+ * reference loss ids.  Returns NaN for an unknown id or a length mismatch. */
+SNN_API float get_loss_all(float *labels, int num_labels, float *predictions, int num_predictions,
+                           int loss_function);
+
+/* ---------------------------------------------------------------------------
+ * 2. Handle API
+ * ------------------------------------------------------------------------- */
+
+typedef struct snn_handle snn_handle;
+
+typedef struct snn_desc {
+    int n_train;          /* neighbour (training) points                               */
+    int n_val;            /* scored (validation) points; 0 selects CV mode over n_train */
+    int p;                /* features                                                  */
+    const int *k_vals;    /* candidate k values (copied at create)                     */
+    int num_k_vals;
+    int backward;         /* 0 forward selection, 1 backward elimination               */
+    int num_features;     /* forward: features to add; backward: features to keep     */
+    int k_fold;           /* CV mode: number of folds (reference fold rule)            */
+    int auto_feature;     /* stop when the error rises (nearest_neighbors_feature_selection.c:446-465) */
+    int device;           /* CUDA device ordinal                                       */
+} snn_desc;
+
+/* Validate the descriptor, pick the device and allocate its buffers
+ * (the committed distance matrix is n_rows x round_up(n_train, 32) floats). */
+SNN_API int snn_create(const snn_desc *desc, snn_handle **out);
+
+/* Copy host inputs to the device (row-major float32).  X_val/y_val are
+ * ignored (may be NULL) in CV mode.  Resets the selection to step 0. */
+SNN_API int snn_load(snn_handle *h, const float *X_train, const float *y_train, const float *X_val,
+                     const float *y_val);
+
+/* Run the whole selection (all greedy steps) on the handle's stream; blocks
+ * until done. */
+SNN_API int snn_run(snn_handle *h);
+
+/* Restart from step 0 with the loaded data (no copies). */
+SNN_API int snn_reset(snn_handle *h);
+
+/* Run one greedy step.  Returns 1 if a step ran, 0 if the selection had
+ * already finished, or a negative status.  Blocks until the step is done. */
+SNN_API int snn_step(snn_handle *h);
+
+/* Warm start / resume: restart from step 0 and commit seq[0..n) in order
+ * (forward: features added; backward: features removed) without scoring
+ * them, as the reference's distance update would have (the counterpart of
+ * compute_distance_matrix_selected, speedynn/lib/cpu.c:269-299 with
+ * selected_only, but in commit order so later steps stay bit-identical).
+ * Their ordering slots are filled, their errors and best k stay 0.
+ * Subsequent snn_step calls continue from step n. */
+SNN_API int snn_commit_sequence(snn_handle *h, const int *seq, int n);
+
+/* Results so far, all optional (NULL skips), arrays of length p, indexed like
+ * the reference outputs: ordering/errors slot i is the step's loop index
+ * (forward: step number; backward: p-1 down to num_features).
+ * errors: FP32 RMSE bit-identical to the reference; errors64: the same
+ * residuals summed in FP64; step_best_k: best k of each step's winner. */
+SNN_API int snn_get_results(snn_handle *h, int *ordering, int *mask, float *errors, double *errors64,
+                            int *step_best_k, int *best_k, int *num_final);
+
+/* Neighbour lists of the most recent step, for inspection: when enabled
+ * before a step, that step keeps idx/dist[n_cand][n_rows][k_max] (candidates
+ * in ascending feature order, listed in cands[n_cand]).  Pass NULL to query
+ * sizes through n_cand/k_max. */
+SNN_API int snn_keep_neighbours(snn_handle *h, int enable);
+SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_max, int *idx, float *dist);
+
+/* Kernel time of the last snn_run/snn_step calls (CUDA events on the handle's
+ * stream): total milliseconds and launches of the candidate-scoring kernel,
+ * of the commit kernel and of everything the selection launched. */
+SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches, double *commit_ms,
+                           int *commit_launches, double *total_ms, int *total_launches);
+
+SNN_API int snn_destroy(snn_handle *h);
+
+/* Message of the last failure on the calling thread ("" if none). */
+SNN_API const char *snn_last_error(void);
+
+/* Library version string. */
+SNN_API const char *snn_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPEEDYNN_B200_H */

@@ -1,0 +1,543 @@
+// snn_api.cu -- host driver and C ABI of libspeedynn_b200.so.
+//
+// The greedy loop of speedynn/lib/nearest_neighbors_feature_selection.c:76-233
+// (backward) and :243-394 (forward) runs here as a fixed sequence of kernel
+// launches per step on one CUDA stream: score -> reduce -> select -> commit.
+// The winner never travels to the host between steps (the select kernel
+// writes it to device state that the commit and the next scoring read), so a
+// whole selection is issued without synchronisation and waited for once.
+#include <float.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/speedynn_b200.h"
+#include "snn_internal.h"
+
+using snn::Bufs;
+using snn::State;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define SNN_CUDA(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(SNN_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                         \
+    } while (0)
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+}  // namespace
+
+struct snn_handle {
+    snn_desc desc{};
+    std::vector<int> kvals;
+    int n_rows = 0, n_cols = 0, p = 0, cv = 0, npf = 1, kmax = 0, nk = 0;
+    int ldc = 0, ldr = 0;
+    int total_steps = 0;
+    int cc = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    // device buffers
+    float *XT = nullptr, *XV = nullptr, *yc = nullptr, *yr = nullptr, *D = nullptr, *pred = nullptr;
+    float *rmse32 = nullptr, *err = nullptr, *stage = nullptr;
+    double *rmse64 = nullptr, *err64 = nullptr;
+    int *kv = nullptr, *cands = nullptr, *prev_cands = nullptr, *mask = nullptr, *order = nullptr, *stepk = nullptr;
+    State *st = nullptr;
+    int *nn_idx = nullptr;
+    float *nn_dist = nullptr;
+    bool keep_nn = false;
+    int nn_ncand = 0;
+    bool loaded = false;
+    int host_step = 0;  // steps issued since the last reset
+    // timing
+    std::vector<EventPair> score_ev, commit_ev;
+    EventPair total_ev;
+    int n_score = 0, n_commit = 0, n_launch = 0;
+
+    Bufs bufs() const
+    {
+        Bufs b;
+        b.XT = XT;
+        b.XV = XV;
+        b.ldc = ldc;
+        b.ldr = ldr;
+        b.yc = yc;
+        b.yr = yr;
+        b.D = D;
+        b.n_rows = n_rows;
+        b.n_cols = n_cols;
+        b.p = p;
+        b.kvals = kv;
+        b.nk = nk;
+        b.kmax = kmax;
+        b.pred = pred;
+        b.rmse32 = rmse32;
+        b.rmse64 = rmse64;
+        b.cands = cands;
+        b.prev_cands = prev_cands;
+        b.mask = mask;
+        b.order = order;
+        b.err = err;
+        b.err64 = err64;
+        b.stepk = stepk;
+        b.st = st;
+        b.nn_idx = keep_nn ? nn_idx : nullptr;
+        b.nn_dist = keep_nn ? nn_dist : nullptr;
+        return b;
+    }
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(T **p, size_t n, const char *what)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? SNN_ERR_NOMEM : SNN_ERR_CUDA,
+                    "cudaMalloc of %s (%zu bytes) failed: %s", what, n * sizeof(T), cudaGetErrorString(e));
+    }
+    return SNN_OK;
+}
+
+void free_all(snn_handle *h)
+{
+    cudaSetDevice(h->device);
+    void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
+                    h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
+                    h->stepk, h->st, h->nn_idx, h->nn_dist};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    for (auto &e : h->score_ev) {
+        if (e.a) cudaEventDestroy(e.a);
+        if (e.b) cudaEventDestroy(e.b);
+    }
+    for (auto &e : h->commit_ev) {
+        if (e.a) cudaEventDestroy(e.a);
+        if (e.b) cudaEventDestroy(e.b);
+    }
+    if (h->total_ev.a) cudaEventDestroy(h->total_ev.a);
+    if (h->total_ev.b) cudaEventDestroy(h->total_ev.b);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+int make_pair(EventPair &e)
+{
+    if (!e.a) SNN_CUDA(cudaEventCreate(&e.a));
+    if (!e.b) SNN_CUDA(cudaEventCreate(&e.b));
+    return SNN_OK;
+}
+
+int check_device(int device)
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(SNN_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= n) return fail(SNN_ERR_ARG, "device %d out of range (%d devices)", device, n);
+    cudaDeviceProp prop;
+    SNN_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(SNN_ERR_CUDA, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                                      prop.major, prop.minor);
+    return SNN_OK;
+}
+
+// Issue one greedy step (no synchronisation).
+int issue_step(snn_handle *h, int t)
+{
+    const Bufs b = h->bufs();
+    const int n_cand = h->p - t;  // forward: p - t unselected; backward: p - t still selected
+    const int backward = h->desc.backward;
+    const int it = backward ? h->p - 1 - t : t;
+    if ((int)h->score_ev.size() <= h->n_score) h->score_ev.resize(h->n_score + 1);
+    EventPair &se = h->score_ev[h->n_score];
+    if (int rc = make_pair(se)) return rc;
+    SNN_CUDA(cudaEventRecord(se.a, h->stream));
+    SNN_CUDA(snn::launch_score(b, n_cand, h->cc, backward, h->stream));
+    SNN_CUDA(cudaEventRecord(se.b, h->stream));
+    h->n_score++;
+    SNN_CUDA(snn::launch_reduce(b, n_cand, h->stream));
+    SNN_CUDA(snn::launch_select(b, n_cand, it, t, h->total_steps, backward, h->desc.auto_feature, h->stream));
+    h->n_launch += 3;
+    if (h->keep_nn) h->nn_ncand = n_cand;
+    if (t + 1 < h->total_steps) {
+        if ((int)h->commit_ev.size() <= h->n_commit) h->commit_ev.resize(h->n_commit + 1);
+        EventPair &ce = h->commit_ev[h->n_commit];
+        if (int rc = make_pair(ce)) return rc;
+        SNN_CUDA(cudaEventRecord(ce.a, h->stream));
+        SNN_CUDA(snn::launch_commit(b, backward, h->stream));
+        SNN_CUDA(cudaEventRecord(ce.b, h->stream));
+        h->n_commit++;
+        h->n_launch += 1;
+    }
+    return SNN_OK;
+}
+
+int issue_reset(snn_handle *h)
+{
+    const Bufs b = h->bufs();
+    SNN_CUDA(snn::launch_reset_state(b, h->desc.backward, h->total_steps, h->stream));
+    if (h->desc.backward)
+        SNN_CUDA(snn::launch_full_distance(b, h->cv, h->npf, h->stream));
+    else
+        SNN_CUDA(snn::launch_init_forward(b, h->cv, h->npf, h->stream));
+    h->n_launch += 2;
+    h->host_step = 0;
+    return SNN_OK;
+}
+
+int read_state(snn_handle *h, State *s)
+{
+    SNN_CUDA(cudaMemcpyAsync(s, h->st, sizeof(State), cudaMemcpyDeviceToHost, h->stream));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    return SNN_OK;
+}
+
+void reset_timing(snn_handle *h)
+{
+    h->n_score = h->n_commit = h->n_launch = 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Handle API
+// ===========================================================================
+extern "C" {
+
+SNN_API const char *snn_last_error(void) { return g_err.c_str(); }
+
+SNN_API const char *snn_version(void) { return "speedynn_b200 0.1.0 (sm_100a)"; }
+
+SNN_API int snn_create(const snn_desc *d, snn_handle **out)
+{
+    g_err.clear();
+    if (!d || !out) return fail(SNN_ERR_ARG, "null descriptor or output pointer");
+    *out = nullptr;
+    if (d->n_train <= 0 || d->p <= 0 || d->n_val < 0) return fail(SNN_ERR_ARG, "bad shape n_train=%d n_val=%d p=%d",
+                                                                 d->n_train, d->n_val, d->p);
+    if (!d->k_vals || d->num_k_vals <= 0) return fail(SNN_ERR_ARG, "k_vals must be a non-empty array");
+    int kmax = 0;
+    for (int m = 0; m < d->num_k_vals; ++m) {
+        if (d->k_vals[m] <= 0) return fail(SNN_ERR_ARG, "k_vals[%d]=%d must be >= 1", m, d->k_vals[m]);
+        kmax = std::max(kmax, d->k_vals[m]);
+    }
+    if (d->num_features < 0 || d->num_features > d->p)
+        return fail(SNN_ERR_ARG, "num_features=%d must lie in [0, p=%d]", d->num_features, d->p);
+    const int cv = d->n_val == 0;
+    if (cv && (d->k_fold <= 0 || d->k_fold > d->n_train))
+        return fail(SNN_ERR_ARG, "k_fold=%d must lie in [1, n=%d]", d->k_fold, d->n_train);
+    if (int rc = check_device(d->device)) return rc;
+
+    snn_handle *h = new snn_handle();
+    h->desc = *d;
+    h->kvals.assign(d->k_vals, d->k_vals + d->num_k_vals);
+    h->desc.k_vals = nullptr;
+    h->device = d->device;
+    h->p = d->p;
+    h->cv = cv;
+    h->n_cols = d->n_train;
+    h->n_rows = cv ? d->n_train : d->n_val;
+    h->npf = cv ? d->n_train / d->k_fold : 1;
+    h->kmax = kmax;
+    h->nk = d->num_k_vals;
+    h->ldc = round_up(h->n_cols, snn::kPadCols);
+    h->ldr = cv ? h->ldc : round_up(h->n_rows, snn::kPadCols);
+    if (d->auto_feature)
+        h->total_steps = d->p;
+    else
+        h->total_steps = d->backward ? d->p - d->num_features : d->num_features;
+
+    int rc = SNN_OK;
+    auto bail = [&](int code) {
+        free_all(h);
+        delete h;
+        return code;
+    };
+    if (cudaSetDevice(h->device) != cudaSuccess) return bail(fail(SNN_ERR_CUDA, "cudaSetDevice(%d) failed", h->device));
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    h->cc = snn::pick_score_cc(kmax, max_smem);
+    if (h->cc == 0) return bail(fail(SNN_ERR_UNSUPPORTED, "k_max=%d needs more shared memory than a block has", kmax));
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(SNN_ERR_CUDA, "cudaStreamCreate failed"));
+
+    const size_t p = (size_t)h->p;
+    if ((rc = dev_alloc(&h->XT, p * h->ldc, "X_train"))) return bail(rc);
+    if ((rc = dev_alloc(&h->yc, (size_t)h->n_cols, "y_train"))) return bail(rc);
+    if (cv) {
+        h->XV = h->XT;
+        h->yr = h->yc;
+    } else {
+        if ((rc = dev_alloc(&h->XV, p * h->ldr, "X_val"))) return bail(rc);
+        if ((rc = dev_alloc(&h->yr, (size_t)h->n_rows, "y_val"))) return bail(rc);
+    }
+    if ((rc = dev_alloc(&h->D, (size_t)h->n_rows * h->ldc, "distance matrix"))) return bail(rc);
+    if ((rc = dev_alloc(&h->pred, p * h->nk * h->n_rows, "predictions"))) return bail(rc);
+    if ((rc = dev_alloc(&h->rmse32, p * h->nk, "errors"))) return bail(rc);
+    if ((rc = dev_alloc(&h->rmse64, p * h->nk, "errors64"))) return bail(rc);
+    if ((rc = dev_alloc(&h->err, p, "step errors"))) return bail(rc);
+    if ((rc = dev_alloc(&h->err64, p, "step errors64"))) return bail(rc);
+    if ((rc = dev_alloc(&h->kv, (size_t)h->nk, "k_vals"))) return bail(rc);
+    if ((rc = dev_alloc(&h->cands, p, "candidates"))) return bail(rc);
+    if ((rc = dev_alloc(&h->prev_cands, p, "candidates"))) return bail(rc);
+    if ((rc = dev_alloc(&h->mask, p, "mask"))) return bail(rc);
+    if ((rc = dev_alloc(&h->order, p, "ordering"))) return bail(rc);
+    if ((rc = dev_alloc(&h->stepk, p, "best k"))) return bail(rc);
+    if ((rc = dev_alloc(&h->st, 1, "state"))) return bail(rc);
+    if (cudaMemcpy(h->kv, h->kvals.data(), sizeof(int) * h->nk, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(SNN_ERR_CUDA, "copy of k_vals failed"));
+    if (make_pair(h->total_ev)) return bail(SNN_ERR_CUDA);
+    *out = h;
+    return SNN_OK;
+}
+
+static int load_matrix(snn_handle *h, const float *X, int n, float *XT, int ld, bool device_src)
+{
+    const size_t bytes = sizeof(float) * (size_t)n * h->p;
+    const float *src = X;
+    if (!device_src) {
+        if (!h->stage) {
+            size_t n_stage = (size_t)std::max(h->n_rows, h->n_cols) * h->p;
+            if (int rc = dev_alloc(&h->stage, n_stage, "staging")) return rc;
+        }
+        SNN_CUDA(cudaMemcpyAsync(h->stage, X, bytes, cudaMemcpyHostToDevice, h->stream));
+        src = h->stage;
+    }
+    SNN_CUDA(snn::launch_transpose(src, n, h->p, XT, ld, h->stream));
+    return SNN_OK;
+}
+
+static int load_impl(snn_handle *h, const float *X_train, const float *y_train, const float *X_val,
+                     const float *y_val, bool device_src)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!X_train || !y_train) return fail(SNN_ERR_ARG, "X_train and y_train are required");
+    if (!h->cv && (!X_val || !y_val)) return fail(SNN_ERR_ARG, "holdout mode needs X_val and y_val");
+    SNN_CUDA(cudaSetDevice(h->device));
+    const cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (int rc = load_matrix(h, X_train, h->n_cols, h->XT, h->ldc, device_src)) return rc;
+    SNN_CUDA(cudaMemcpyAsync(h->yc, y_train, sizeof(float) * h->n_cols, kind, h->stream));
+    if (!h->cv) {
+        // the staging buffer is reused: order the second upload after the first transpose
+        if (int rc = load_matrix(h, X_val, h->n_rows, h->XV, h->ldr, device_src)) return rc;
+        SNN_CUDA(cudaMemcpyAsync(h->yr, y_val, sizeof(float) * h->n_rows, kind, h->stream));
+    }
+    h->loaded = true;
+    reset_timing(h);
+    if (int rc = issue_reset(h)) return rc;
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    return SNN_OK;
+}
+
+SNN_API int snn_load(snn_handle *h, const float *X_train, const float *y_train, const float *X_val, const float *y_val)
+{
+    return load_impl(h, X_train, y_train, X_val, y_val, false);
+}
+
+SNN_API int snn_reset(snn_handle *h)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!h->loaded) return fail(SNN_ERR_STATE, "snn_reset before snn_load");
+    SNN_CUDA(cudaSetDevice(h->device));
+    reset_timing(h);
+    if (int rc = issue_reset(h)) return rc;
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    return SNN_OK;
+}
+
+SNN_API int snn_run(snn_handle *h)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!h->loaded) return fail(SNN_ERR_STATE, "snn_run before snn_load");
+    SNN_CUDA(cudaSetDevice(h->device));
+    reset_timing(h);
+    SNN_CUDA(cudaEventRecord(h->total_ev.a, h->stream));
+    // every run is a complete selection from the initial distance matrix
+    if (int rc = issue_reset(h)) return rc;
+    for (int t = 0; t < h->total_steps; ++t)
+        if (int rc = issue_step(h, t)) return rc;
+    h->host_step = h->total_steps;
+    SNN_CUDA(cudaEventRecord(h->total_ev.b, h->stream));
+    State s;
+    if (int rc = read_state(h, &s)) return rc;
+    if (s.error) return fail(s.error, "no candidate had an error below FLT_MAX at step %d (non-finite labels?)", s.step);
+    return SNN_OK;
+}
+
+SNN_API int snn_step(snn_handle *h)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!h->loaded) return fail(SNN_ERR_STATE, "snn_step before snn_load");
+    SNN_CUDA(cudaSetDevice(h->device));
+    State s;
+    if (int rc = read_state(h, &s)) return rc;
+    if (s.error) return fail(s.error, "selection stopped with an error at step %d", s.step);
+    if (s.done || h->host_step >= h->total_steps) return 0;
+    reset_timing(h);
+    SNN_CUDA(cudaEventRecord(h->total_ev.a, h->stream));
+    if (int rc = issue_step(h, h->host_step)) return rc;
+    SNN_CUDA(cudaEventRecord(h->total_ev.b, h->stream));
+    h->host_step++;
+    if (int rc = read_state(h, &s)) return rc;
+    if (s.error) return fail(s.error, "no candidate had an error below FLT_MAX at step %d", s.step);
+    return 1;
+}
+
+SNN_API int snn_commit_sequence(snn_handle *h, const int *seq, int n)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!h->loaded) return fail(SNN_ERR_STATE, "snn_commit_sequence before snn_load");
+    if (n < 0 || n > h->total_steps || (n > 0 && !seq))
+        return fail(SNN_ERR_ARG, "sequence length %d outside [0, %d]", n, h->total_steps);
+    std::vector<char> used(h->p, 0);
+    for (int i = 0; i < n; ++i) {
+        if (seq[i] < 0 || seq[i] >= h->p || used[seq[i]])
+            return fail(SNN_ERR_ARG, "sequence entry %d (=%d) is out of range or repeated", i, seq[i]);
+        used[seq[i]] = 1;
+    }
+    SNN_CUDA(cudaSetDevice(h->device));
+    reset_timing(h);
+    if (int rc = issue_reset(h)) return rc;
+    const Bufs b = h->bufs();
+    for (int t = 0; t < n; ++t) {
+        const int it = h->desc.backward ? h->p - 1 - t : t;
+        SNN_CUDA(snn::launch_force(b, seq[t], it, t, h->total_steps, h->desc.backward, h->stream));
+        SNN_CUDA(snn::launch_commit(b, h->desc.backward, h->stream));
+    }
+    h->host_step = n;
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    return SNN_OK;
+}
+
+SNN_API int snn_get_results(snn_handle *h, int *ordering, int *mask, float *errors, double *errors64, int *step_best_k,
+                            int *best_k, int *num_final)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    SNN_CUDA(cudaSetDevice(h->device));
+    const size_t p = (size_t)h->p;
+    if (ordering) SNN_CUDA(cudaMemcpyAsync(ordering, h->order, p * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (mask) SNN_CUDA(cudaMemcpyAsync(mask, h->mask, p * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (errors) SNN_CUDA(cudaMemcpyAsync(errors, h->err, p * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    if (errors64) SNN_CUDA(cudaMemcpyAsync(errors64, h->err64, p * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (step_best_k) SNN_CUDA(cudaMemcpyAsync(step_best_k, h->stepk, p * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    State s;
+    if (int rc = read_state(h, &s)) return rc;
+    if (best_k) *best_k = s.best_k_last;
+    if (num_final) *num_final = s.num_final;
+    return SNN_OK;
+}
+
+SNN_API int snn_keep_neighbours(snn_handle *h, int enable)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    SNN_CUDA(cudaSetDevice(h->device));
+    if (enable && !h->nn_idx) {
+        const size_t n = (size_t)h->p * h->n_rows * h->kmax;
+        if (int rc = dev_alloc(&h->nn_idx, n, "neighbour indices")) return rc;
+        if (int rc = dev_alloc(&h->nn_dist, n, "neighbour distances")) return rc;
+    }
+    h->keep_nn = enable != 0;
+    h->nn_ncand = 0;
+    return SNN_OK;
+}
+
+SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_max, int *idx, float *dist)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!h->keep_nn || h->nn_ncand == 0) return fail(SNN_ERR_STATE, "no neighbour lists kept (snn_keep_neighbours)");
+    SNN_CUDA(cudaSetDevice(h->device));
+    if (n_cand) *n_cand = h->nn_ncand;
+    if (k_max) *k_max = h->kmax;
+    const size_t n = (size_t)h->nn_ncand * h->n_rows * h->kmax;
+    if (cands) SNN_CUDA(cudaMemcpyAsync(cands, h->prev_cands, sizeof(int) * h->nn_ncand, cudaMemcpyDeviceToHost, h->stream));
+    if (idx) SNN_CUDA(cudaMemcpyAsync(idx, h->nn_idx, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    if (dist) SNN_CUDA(cudaMemcpyAsync(dist, h->nn_dist, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    return SNN_OK;
+}
+
+SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches, double *commit_ms, int *commit_launches,
+                           double *total_ms, int *total_launches)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    SNN_CUDA(cudaSetDevice(h->device));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    double s = 0.0, c = 0.0;
+    for (int i = 0; i < h->n_score; ++i) {
+        float ms = 0.f;
+        SNN_CUDA(cudaEventElapsedTime(&ms, h->score_ev[i].a, h->score_ev[i].b));
+        s += ms;
+    }
+    for (int i = 0; i < h->n_commit; ++i) {
+        float ms = 0.f;
+        SNN_CUDA(cudaEventElapsedTime(&ms, h->commit_ev[i].a, h->commit_ev[i].b));
+        c += ms;
+    }
+    float tot = 0.f;
+    if (h->n_launch > 0) {
+        cudaError_t e = cudaEventElapsedTime(&tot, h->total_ev.a, h->total_ev.b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            tot = 0.f;
+        }
+    }
+    if (score_ms) *score_ms = s;
+    if (score_launches) *score_launches = h->n_score;
+    if (commit_ms) *commit_ms = c;
+    if (commit_launches) *commit_launches = h->n_commit;
+    if (total_ms) *total_ms = tot;
+    if (total_launches) *total_launches = h->n_launch;
+    return SNN_OK;
+}
+
+SNN_API int snn_destroy(snn_handle *h)
+{
+    if (!h) return SNN_OK;
+    free_all(h);
+    delete h;
+    return SNN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// Internal declarations shared by the kernels (snn_kernels.cu) and the host
+// driver (snn_api.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace snn {
+
+// Selection state kept on the device so that a whole greedy step (score ->
+// reduce -> select -> commit) runs without a host round trip.
+struct State {
+    int step;         // greedy steps completed
+    int done;         // 1: selection finished (last step, auto stop or error)
+    int error;        // SNN_ERR_NO_WINNER when no candidate had a finite error
+    int winner;       // feature chosen by the last completed step
+    int n_cand;       // candidates of the next step
+    int best_k_last;  // best k of the last winner
+    int num_final;    // features in the model after the last step
+    int pad;
+};
+
+// Everything a kernel needs, passed by value.
+//
+// Layout in HBM:
+//   XT  [p][ldc]  neighbour (training) points, feature-major, zero padded
+//   XV  [p][ldr]  scored points, feature-major (aliases XT in CV mode)
+//   D   [n_rows][ldc]  committed FP32 distance matrix, row = scored point;
+//                 +inf on excluded pairs (same CV fold) and on pad columns
+//   pred [p][nk][n_rows]  kNN-mean prediction per (candidate slot, k, row)
+struct Bufs {
+    const float *XT;
+    const float *XV;
+    int ldc, ldr;
+    const float *yc;
+    const float *yr;
+    float *D;
+    int n_rows, n_cols, p;
+    const int *kvals;
+    int nk, kmax;
+    float *pred;
+    float *rmse32;
+    double *rmse64;
+    int *cands;       // current candidate list (ascending feature ids)
+    int *prev_cands;  // candidate list of the last scored step
+    int *mask;
+    int *order;
+    float *err;
+    double *err64;
+    int *stepk;
+    State *st;
+    int *nn_idx;      // optional [n_cand][n_rows][kmax]
+    float *nn_dist;
+};
+
+constexpr int kScoreRows = 128;  // rows (threads) per scoring block
+constexpr int kTileCols = 32;    // columns per D tile
+constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D
+
+size_t score_smem_bytes(int cc, int kmax);
+int pick_score_cc(int kmax, int max_smem);
+
+cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);
+cudaError_t launch_init_forward(const Bufs &b, int cv, int npf, cudaStream_t s);
+cudaError_t launch_full_distance(const Bufs &b, int cv, int npf, cudaStream_t s);
+cudaError_t launch_score(const Bufs &b, int n_cand, int cc, int backward, cudaStream_t s);
+cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s);
+cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_steps, int backward,
+                          int auto_feature, cudaStream_t s);
+cudaError_t launch_commit(const Bufs &b, int backward, cudaStream_t s);
+cudaError_t launch_reset_state(const Bufs &b, int backward, int total_steps, cudaStream_t s);
+cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s);
+
+}  // namespace snn

@@ -1,0 +1,600 @@
+// snn_kernels.cu -- sm_100a kernels of one greedy feature-selection step.
+//
+// Arithmetic contract (bit parity with speedynn's CPU path):
+//   candidate distance  d = D[r,i] +/- fl(fl(x_r,c - x_i,c)^2)
+//                       (speedynn/lib/cpu.c:226-228, util.c:19-21), every op
+//                       rounded separately: __fsub_rn/__fmul_rn/__fadd_rn keep
+//                       the compiler from contracting into FMA;
+//   neighbour list      stable (distance, index) order of the items with
+//                       distance < FLT_MAX, padded with (FLT_MAX, 0)
+//                       (cpu.c:212-252);
+//   prediction          FP32 label sum in rank order, then / k (cpu.c:140-150);
+//   RMSE                FP32 sequential sum over rows, / n, sqrt in double,
+//                       rounded to float (loss_functions.c:41-50);
+//   committed distance  forward fl(D + s_w) in selection order
+//                       (cpu.c:301-315); backward: full distance summed over
+//                       dims in descending order (util.c:10-17), then
+//                       fl(D - s_w) in removal order.
+#include <float.h>
+#include <math.h>
+
+#include "snn_internal.h"
+
+namespace snn {
+
+namespace {
+
+__device__ __forceinline__ float sqdiff(float a, float b)
+{
+    const float t = __fsub_rn(a, b);
+    return __fmul_rn(t, t);
+}
+
+// ---------------------------------------------------------------------------
+// Row-major [n][p] -> feature-major [p][ld], zero padded up to ld.
+// ---------------------------------------------------------------------------
+__global__ void k_transpose(const float *__restrict__ X, int n, int p, float *__restrict__ XT, int ld)
+{
+    __shared__ float tile[32][33];
+    const int i0 = blockIdx.x * 32;  // points
+    const int f0 = blockIdx.y * 32;  // features
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int i = i0 + k, f = f0 + threadIdx.x;
+        tile[k][threadIdx.x] = (i < n && f < p) ? X[(size_t)i * p + f] : 0.0f;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int f = f0 + k, i = i0 + threadIdx.x;
+        if (f < p && i < ld) XT[(size_t)f * ld + i] = tile[threadIdx.x][k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Forward start: D = 0 on scored pairs, +inf on excluded / pad columns
+// (speedynn/lib/cpu.c:255-267 zero-fills; exclusion is the fold rule of
+// cpu.c:223 folded into the matrix so the scoring loop needs no test).
+// ---------------------------------------------------------------------------
+__global__ void k_init_forward(Bufs b, int cv, int npf)
+{
+    const int ld4 = b.ldc >> 2;
+    for (int r = blockIdx.x; r < b.n_rows; r += gridDim.x) {
+        const int lo = cv ? (r / npf) * npf : 0;
+        float4 *row = reinterpret_cast<float4 *>(b.D + (size_t)r * b.ldc);
+        for (int q = threadIdx.x; q < ld4; q += blockDim.x) {
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int i = q * 4 + e;
+                const bool ex = (i >= b.n_cols) || (cv && (unsigned)(i - lo) < (unsigned)npf);
+                v[e] = ex ? INFINITY : 0.0f;
+            }
+            row[q] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Backward start: full distance over all p dims, summed in DESCENDING
+// dimension order (speedynn/lib/util.c:10-17).  64x64 output tile per block,
+// 4x4 per thread, features streamed through shared memory in chunks.
+// ---------------------------------------------------------------------------
+constexpr int kFdTile = 64;
+constexpr int kFdChunk = 16;
+
+__global__ void __launch_bounds__(256) k_full_distance(Bufs b, int cv, int npf)
+{
+    __shared__ __align__(16) float sv[kFdChunk][kFdTile];
+    __shared__ __align__(16) float sc[kFdChunk][kFdTile];
+    const int r0 = blockIdx.y * kFdTile;
+    const int i0 = blockIdx.x * kFdTile;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0f;
+
+    for (int kk = b.p; kk > 0; kk -= kFdChunk) {
+        const int kb = kk > kFdChunk ? kk - kFdChunk : 0;
+        const int cnt = kk - kb;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kFdChunk * kFdTile; e += blockDim.x) {
+            const int q = e / kFdTile, x = e % kFdTile;
+            float a = 0.0f, c = 0.0f;
+            if (q < cnt) {
+                a = b.XV[(size_t)(kb + q) * b.ldr + r0 + x];  // ldr, ldc are multiples of 64
+                c = b.XT[(size_t)(kb + q) * b.ldc + i0 + x];
+            }
+            sv[q][x] = a;
+            sc[q][x] = c;
+        }
+        __syncthreads();
+        for (int q = cnt - 1; q >= 0; --q) {
+            const float4 a4 = *reinterpret_cast<const float4 *>(&sv[q][ty * 4]);
+            const float4 c4 = *reinterpret_cast<const float4 *>(&sc[q][tx * 4]);
+            const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+            const float c[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = __fadd_rn(acc[u][v], sqdiff(a[u], c[v]));
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int r = r0 + ty * 4 + u;
+        if (r >= b.n_rows) continue;
+        const int lo = cv ? (r / npf) * npf : 0;
+        float v4[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int i = i0 + tx * 4 + v;
+            const bool ex = (i >= b.n_cols) || (cv && (unsigned)(i - lo) < (unsigned)npf);
+            v4[v] = ex ? INFINITY : acc[u][v];
+        }
+        *reinterpret_cast<float4 *>(b.D + (size_t)r * b.ldc + i0 + tx * 4) = make_float4(v4[0], v4[1], v4[2], v4[3]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Candidate scoring (the hot kernel).
+//
+// One thread owns one scored row r and CC candidate features; a block owns
+// 128 rows and one chunk of CC candidates and streams the row block of D
+// through shared memory in 32-column tiles (coalesced float4 loads, register
+// prefetch of the next tile, stored transposed so each thread reads its own
+// row conflict-free).  The candidate columns of X for the tile sit in shared
+// memory and are read as broadcasts; x_r,c lives in registers.  Each
+// (row, candidate) keeps its top-k_max list in shared memory, interleaved by
+// thread, with the k-th distance cached in a register as the entry test.
+// The epilogue forms the kNN-mean predictions for every k of k_vals.
+// ---------------------------------------------------------------------------
+constexpr int kDsLd = kScoreRows + 1;
+
+__device__ __forceinline__ float list_insert(float *Ld, int *Li, int base, int K, float d, int i)
+{
+    int pos = K - 1;
+    while (pos > 0) {
+        const float prev = Ld[base + (pos - 1) * kScoreRows];
+        if (!(prev > d)) break;
+        Ld[base + pos * kScoreRows] = prev;
+        Li[base + pos * kScoreRows] = Li[base + (pos - 1) * kScoreRows];
+        --pos;
+    }
+    Ld[base + pos * kScoreRows] = d;
+    Li[base + pos * kScoreRows] = i;
+    return Ld[base + (K - 1) * kScoreRows];
+}
+
+template <int CC, bool BWD>
+__global__ void __launch_bounds__(kScoreRows) k_score(Bufs b, int n_cand, int n_chunks)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *Ds = reinterpret_cast<float *>(smem_raw);           // [kTileCols][kDsLd]
+    float *Xs = Ds + kTileCols * kDsLd;                          // [kTileCols][CC]
+    int *scand = reinterpret_cast<int *>(Xs + kTileCols * CC);   // [CC]
+    float *Ld = reinterpret_cast<float *>(scand + CC);           // [CC][K][kScoreRows]
+    const int K = b.kmax;
+    int *Li = reinterpret_cast<int *>(Ld + (size_t)CC * K * kScoreRows);
+
+    if (b.st->done) return;
+
+    const int tid = threadIdx.x;
+    const int chunk = blockIdx.x % n_chunks;
+    const int r0 = (blockIdx.x / n_chunks) * kScoreRows;
+    const int r = r0 + tid;
+    const bool rvalid = r < b.n_rows;
+    const int c0 = chunk * CC;
+
+    if (tid < CC) {
+        const int ci = c0 + tid;
+        scand[tid] = b.cands[ci < n_cand ? ci : 0];
+    }
+    __syncthreads();
+
+    float xv[CC], thr[CC];
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+        xv[c] = rvalid ? b.XV[(size_t)scand[c] * b.ldr + r] : 0.0f;
+        thr[c] = FLT_MAX;
+    }
+    for (int c = 0; c < CC; ++c)
+        for (int j = 0; j < K; ++j) {
+            Ld[(c * K + j) * kScoreRows + tid] = FLT_MAX;
+            Li[(c * K + j) * kScoreRows + tid] = 0;
+        }
+
+    // tile loaders: 128 rows x 32 cols of D = 1024 float4, 8 per thread;
+    // CC x 32 candidate values = CC*8 float4.
+    float4 dreg[8];
+    float4 xreg = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto load_tile = [&](int tile) {
+        const int i0 = tile * kTileCols;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int f = tid + kScoreRows * q;
+            const int row = f >> 3, c4 = f & 7;
+            if (r0 + row < b.n_rows)
+                dreg[q] = __ldcs(reinterpret_cast<const float4 *>(b.D + (size_t)(r0 + row) * b.ldc + i0 + c4 * 4));
+            else
+                dreg[q] = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+        }
+        if (tid < CC * 8) {
+            const int c = tid >> 3, c4 = tid & 7;
+            xreg = __ldg(reinterpret_cast<const float4 *>(b.XT + (size_t)scand[c] * b.ldc + i0 + c4 * 4));
+        }
+    };
+    auto store_tile = [&]() {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int f = tid + kScoreRows * q;
+            const int row = f >> 3, c4 = f & 7;
+            Ds[(c4 * 4 + 0) * kDsLd + row] = dreg[q].x;
+            Ds[(c4 * 4 + 1) * kDsLd + row] = dreg[q].y;
+            Ds[(c4 * 4 + 2) * kDsLd + row] = dreg[q].z;
+            Ds[(c4 * 4 + 3) * kDsLd + row] = dreg[q].w;
+        }
+        if (tid < CC * 8) {
+            const int c = tid >> 3, c4 = tid & 7;
+            Xs[(c4 * 4 + 0) * CC + c] = xreg.x;
+            Xs[(c4 * 4 + 1) * CC + c] = xreg.y;
+            Xs[(c4 * 4 + 2) * CC + c] = xreg.z;
+            Xs[(c4 * 4 + 3) * CC + c] = xreg.w;
+        }
+    };
+
+    const int ntiles = b.ldc / kTileCols;
+    load_tile(0);
+    for (int tile = 0; tile < ntiles; ++tile) {
+        __syncthreads();
+        store_tile();
+        __syncthreads();
+        if (tile + 1 < ntiles) load_tile(tile + 1);
+        if (rvalid) {
+            const int i0 = tile * kTileCols;
+#pragma unroll 2
+            for (int j = 0; j < kTileCols; ++j) {
+                const float dv = Ds[j * kDsLd + tid];
+#pragma unroll
+                for (int c = 0; c < CC; ++c) {
+                    const float s = sqdiff(xv[c], Xs[j * CC + c]);
+                    const float d = BWD ? __fsub_rn(dv, s) : __fadd_rn(dv, s);
+                    if (d < thr[c]) thr[c] = list_insert(Ld, Li, c * K * kScoreRows + tid, K, d, i0 + j);
+                }
+            }
+        }
+    }
+
+    if (!rvalid) return;
+#pragma unroll
+    for (int c = 0; c < CC; ++c) {
+        const int slot = c0 + c;
+        if (slot >= n_cand) continue;
+        const int base = c * K * kScoreRows + tid;
+        if (b.nn_idx) {
+            const size_t o = ((size_t)slot * b.n_rows + r) * K;
+            for (int j = 0; j < K; ++j) {
+                b.nn_idx[o + j] = Li[base + j * kScoreRows];
+                b.nn_dist[o + j] = Ld[base + j * kScoreRows];
+            }
+        }
+        // label prefix sums in rank order, in place of the distances
+        float acc = 0.0f;
+        for (int j = 0; j < K; ++j) {
+            acc = __fadd_rn(acc, __ldg(b.yc + Li[base + j * kScoreRows]));
+            Ld[base + j * kScoreRows] = acc;
+        }
+        for (int m = 0; m < b.nk; ++m) {
+            const int k = __ldg(b.kvals + m);
+            b.pred[((size_t)slot * b.nk + m) * b.n_rows + r] = __fdiv_rn(Ld[base + (k - 1) * kScoreRows], (float)k);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per (candidate, k) error: one warp per pair.  Lanes form the squared
+// residuals in parallel; lane 0 adds them in row order in FP32 (the
+// reference's sequential sum); every lane also accumulates its residuals in
+// FP64, combined by a fixed shuffle tree (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kReduceWarps = 4;
+constexpr int kReduceChunk = 256;
+
+__global__ void __launch_bounds__(kReduceWarps * 32) k_reduce(Bufs b, int n_cand)
+{
+    __shared__ float sq[kReduceWarps][kReduceChunk];
+    if (b.st->done) return;
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * kReduceWarps + wl;
+    if (w >= n_cand * b.nk) return;
+    const float *pr = b.pred + (size_t)w * b.n_rows;
+    float s32 = 0.0f;
+    double s64 = 0.0;
+    for (int base = 0; base < b.n_rows; base += kReduceChunk) {
+#pragma unroll
+        for (int q = 0; q < kReduceChunk / 32; ++q) {
+            const int rr = base + q * 32 + lane;
+            if (rr < b.n_rows) {
+                const float pv = pr[rr];
+                const float yv = b.yr[rr];
+                const float e = __fsub_rn(yv, pv);
+                sq[wl][q * 32 + lane] = __fmul_rn(e, e);
+                const double e64 = (double)yv - (double)pv;
+                s64 += e64 * e64;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int cnt = min(kReduceChunk, b.n_rows - base);
+            for (int t = 0; t < cnt; ++t) s32 = __fadd_rn(s32, sq[wl][t]);
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s64 += __shfl_down_sync(0xffffffffu, s64, off);
+    if (lane == 0) {
+        const float mean = __fdiv_rn(s32, (float)b.n_rows);
+        b.rmse32[w] = __double2float_rn(sqrt((double)mean));
+        b.rmse64[w] = sqrt(s64 / (double)b.n_rows);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Best k per candidate (first strict minimum in k_vals order, cpu.c:194-204),
+// best candidate (first strict minimum in ascending feature order,
+// nearest_neighbors_feature_selection.c:155-167 / :318-329), bookkeeping as in
+// :169-181 / :331-342, next candidate list, auto stop (:446-465).
+// ---------------------------------------------------------------------------
+__global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int backward, int auto_feature)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State *st = b.st;
+    if (st->done) return;
+    float minv = FLT_MAX;
+    double min64 = 0.0;
+    int wi = -1, wk = 0;
+    for (int ci = 0; ci < n_cand; ++ci) {
+        float best = FLT_MAX;
+        int bm = -1;
+        for (int m = 0; m < b.nk; ++m) {
+            const float e = b.rmse32[ci * b.nk + m];
+            if (e < best) {
+                best = e;
+                bm = m;
+            }
+        }
+        if (bm < 0) continue;
+        if (best < minv) {
+            minv = best;
+            wi = ci;
+            wk = b.kvals[bm];
+            min64 = b.rmse64[ci * b.nk + bm];
+        }
+    }
+    for (int ci = 0; ci < n_cand; ++ci) b.prev_cands[ci] = b.cands[ci];
+    if (wi < 0) {
+        st->error = -5;  // SNN_ERR_NO_WINNER
+        st->done = 1;
+        return;
+    }
+    const int wdim = b.cands[wi];
+    st->winner = wdim;
+    b.order[it] = wdim;
+    b.err[it] = minv;
+    b.err64[it] = min64;
+    b.stepk[it] = wk;
+    st->best_k_last = wk;
+    b.mask[wdim] = backward ? 0 : 1;
+    st->num_final = backward ? b.p - (t + 1) : t + 1;
+    st->step = t + 1;
+    int nc = 0;
+    for (int j = 0; j < b.p; ++j)
+        if (b.mask[j] == (backward ? 1 : 0)) b.cands[nc++] = j;
+    st->n_cand = nc;
+    if (auto_feature) {
+        if (!backward) {
+            if (it > 0 && b.err[it - 1] < b.err[it]) st->done = 1;
+        } else {
+            if (it > 0 && it < b.p - 1 && b.err[it + 1] < b.err[it]) st->done = 1;
+        }
+    }
+    if (t + 1 >= total_steps) st->done = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Commit the winner into D in place: D = fl(D +/- fl(fl(x_r,w - x_i,w)^2))
+// (speedynn/lib/cpu.c:301-315).  HBM-bound: one read + one write per entry.
+// Excluded / pad entries stay +inf.
+// ---------------------------------------------------------------------------
+template <bool BWD>
+__global__ void __launch_bounds__(256) k_commit(Bufs b)
+{
+    if (b.st->done) return;
+    const int w = b.st->winner;
+    const float *xt = b.XT + (size_t)w * b.ldc;
+    const float *xv = b.XV + (size_t)w * b.ldr;
+    const int ld4 = b.ldc >> 2;
+    for (int r = blockIdx.x; r < b.n_rows; r += gridDim.x) {
+        const float a = __ldg(xv + r);
+        float4 *row = reinterpret_cast<float4 *>(b.D + (size_t)r * b.ldc);
+        for (int q = threadIdx.x; q < ld4; q += blockDim.x) {
+            const float4 c = __ldg(reinterpret_cast<const float4 *>(xt) + q);
+            float4 d = __ldcs(row + q);
+            if (BWD) {
+                d.x = __fsub_rn(d.x, sqdiff(a, c.x));
+                d.y = __fsub_rn(d.y, sqdiff(a, c.y));
+                d.z = __fsub_rn(d.z, sqdiff(a, c.z));
+                d.w = __fsub_rn(d.w, sqdiff(a, c.w));
+            } else {
+                d.x = __fadd_rn(d.x, sqdiff(a, c.x));
+                d.y = __fadd_rn(d.y, sqdiff(a, c.y));
+                d.z = __fadd_rn(d.z, sqdiff(a, c.z));
+                d.w = __fadd_rn(d.w, sqdiff(a, c.w));
+            }
+            __stcs(row + q, d);
+        }
+    }
+}
+
+// Warm start: record a given winner without scoring (same bookkeeping as
+// k_select), so the commit kernel and later steps see it.
+__global__ void k_force(Bufs b, int w, int it, int t, int total_steps, int backward)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    State *st = b.st;
+    st->winner = w;
+    b.order[it] = w;
+    b.err[it] = 0.0f;
+    b.err64[it] = 0.0;
+    b.stepk[it] = 0;
+    b.mask[w] = backward ? 0 : 1;
+    st->num_final = backward ? b.p - (t + 1) : t + 1;
+    st->step = t + 1;
+    int nc = 0;
+    for (int j = 0; j < b.p; ++j)
+        if (b.mask[j] == (backward ? 1 : 0)) b.cands[nc++] = j;
+    st->n_cand = nc;
+    if (t + 1 >= total_steps) st->done = 1;
+}
+
+__global__ void k_reset_state(Bufs b, int backward, int total_steps)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < b.p) {
+        b.mask[j] = backward ? 1 : 0;
+        b.order[j] = 0;
+        b.err[j] = 0.0f;
+        b.err64[j] = 0.0;
+        b.stepk[j] = 0;
+        b.cands[j] = j;
+        b.prev_cands[j] = j;
+    }
+    if (j == 0) {
+        State s;
+        s.step = 0;
+        s.done = total_steps <= 0 ? 1 : 0;
+        s.error = 0;
+        s.winner = -1;
+        s.n_cand = b.p;
+        s.best_k_last = 0;
+        s.num_final = backward ? b.p : 0;
+        s.pad = 0;
+        *b.st = s;
+    }
+}
+
+int sm_count()
+{
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+}  // namespace
+
+size_t score_smem_bytes(int cc, int kmax)
+{
+    return sizeof(float) * (size_t)kTileCols * kDsLd + sizeof(float) * (size_t)kTileCols * cc + sizeof(int) * (size_t)cc +
+           (sizeof(float) + sizeof(int)) * (size_t)cc * kmax * kScoreRows;
+}
+
+int pick_score_cc(int kmax, int max_smem)
+{
+    const int ccs[4] = {8, 4, 2, 1};
+    for (int i = 0; i < 4; ++i)
+        if (score_smem_bytes(ccs[i], kmax) <= (size_t)max_smem) return ccs[i];
+    return 0;
+}
+
+cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s)
+{
+    dim3 grid((ld + 31) / 32, (p + 31) / 32);
+    k_transpose<<<grid, dim3(32, 8), 0, s>>>(X, n, p, XT, ld);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_forward(const Bufs &b, int cv, int npf, cudaStream_t s)
+{
+    int grid = b.n_rows < sm_count() * 8 ? b.n_rows : sm_count() * 8;
+    k_init_forward<<<grid, 256, 0, s>>>(b, cv, npf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_full_distance(const Bufs &b, int cv, int npf, cudaStream_t s)
+{
+    dim3 grid(b.ldc / kFdTile, (b.n_rows + kFdTile - 1) / kFdTile);
+    k_full_distance<<<grid, 256, 0, s>>>(b, cv, npf);
+    return cudaGetLastError();
+}
+
+template <int CC>
+static cudaError_t launch_score_cc(const Bufs &b, int n_cand, int backward, cudaStream_t s)
+{
+    const int n_chunks = (n_cand + CC - 1) / CC;
+    const int n_rb = (b.n_rows + kScoreRows - 1) / kScoreRows;
+    const size_t smem = score_smem_bytes(CC, b.kmax);
+    const long long blocks = (long long)n_chunks * n_rb;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    if (backward) {
+        cudaFuncSetAttribute(k_score<CC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_score<CC, true><<<(unsigned)blocks, kScoreRows, smem, s>>>(b, n_cand, n_chunks);
+    } else {
+        cudaFuncSetAttribute(k_score<CC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_score<CC, false><<<(unsigned)blocks, kScoreRows, smem, s>>>(b, n_cand, n_chunks);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_score(const Bufs &b, int n_cand, int cc, int backward, cudaStream_t s)
+{
+    switch (cc) {
+    case 8: return launch_score_cc<8>(b, n_cand, backward, s);
+    case 4: return launch_score_cc<4>(b, n_cand, backward, s);
+    case 2: return launch_score_cc<2>(b, n_cand, backward, s);
+    case 1: return launch_score_cc<1>(b, n_cand, backward, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s)
+{
+    const int pairs = n_cand * b.nk;
+    k_reduce<<<(pairs + kReduceWarps - 1) / kReduceWarps, kReduceWarps * 32, 0, s>>>(b, n_cand);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_steps, int backward, int auto_feature,
+                          cudaStream_t s)
+{
+    k_select<<<1, 32, 0, s>>>(b, n_cand, it, t, total_steps, backward, auto_feature);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_commit(const Bufs &b, int backward, cudaStream_t s)
+{
+    int grid = b.n_rows < sm_count() * 8 ? b.n_rows : sm_count() * 8;
+    if (backward)
+        k_commit<true><<<grid, 256, 0, s>>>(b);
+    else
+        k_commit<false><<<grid, 256, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s)
+{
+    k_force<<<1, 32, 0, s>>>(b, w, it, t, total_steps, backward);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_state(const Bufs &b, int backward, int total_steps, cudaStream_t s)
+{
+    k_reset_state<<<(b.p + 127) / 128, 128, 0, s>>>(b, backward, total_steps);
+    return cudaGetLastError();
+}
+
+}  // namespace snn

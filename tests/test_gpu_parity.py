@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path against the reference's golden vectors and the
+CPU oracle.  Bar: ordering, mask, best k and neighbour indices bit-exact;
+FP32 errors bit-exact (the reference's own FP32 RMSE); FP64 errors within
+1e-9 relative of the oracle's FP64 sum of the same residuals."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_cases
+from oracle import oracle
+from speedynn_b200 import _lib, datagen
+from speedynn_b200._lib import _f32p, _i32p, ptr
+from speedynn_b200.base import IncrementalNNFeatureSelection
+from speedynn_b200.selector import Selector
+
+pytestmark = pytest.mark.gpu
+
+GDIR = os.path.join(ROOT, "tests", "golden")
+SELECT_CASES = [n for n in golden_cases() if not n.startswith("nn_") and n != "losses"]
+NN_CASES = golden_cases("nn_")
+ERR64_RTOL = 1e-9
+
+
+def _g(name):
+    return dict(np.load(os.path.join(GDIR, name + ".npz")))
+
+
+@pytest.mark.parametrize("name", SELECT_CASES)
+def test_dropin_api_matches_reference_golden(name):
+    g = _g(name)
+    sel = IncrementalNNFeatureSelection(g["X"], g["y"], k_vals=list(g["k_vals"]), auto_feature=bool(g["auto_feature"]),
+                                        num_features=int(g["num_features"]), k_fold=int(g["k_fold"]),
+                                        method=str(g["method"]))
+    sel.train()
+    np.testing.assert_array_equal(sel.get_selected_ordering(), g["ordering"])
+    np.testing.assert_array_equal(sel.get_selected_dimensions(), g["mask"])
+    np.testing.assert_array_equal(sel.get_selected_errors()[:, 0], g["errors"])
+    assert sel.get_optimal_model_k() == int(g["best_k"])
+    assert sel.num_final_features == int(g["num_final"])
+
+
+@pytest.mark.parametrize("name", ["pooled_fwd_3000", "bwd_default_k", "quantized_ties_bwd", "auto_backward"])
+def test_c_abi_reference_entry_points(name):
+    """The SWIG-level names, called through ctypes exactly as the reference's wrapper would."""
+    g = _g(name)
+    L = _lib.lib()
+    X = np.ascontiguousarray(g["X"], np.float32)
+    y = np.ascontiguousarray(g["y"], np.float32)
+    kv = np.ascontiguousarray(g["k_vals"], np.int32)
+    lf = np.zeros(1, np.int32)
+    n, d = X.shape
+    fn = L.train_forward_selection if str(g["method"]) == "forward" else L.train_backward_selection
+    nf = int(g["num_features"]) if not int(g["auto_feature"]) else d
+    rc = fn(ptr(X, _f32p), n, d, ptr(y, _f32p), n, ptr(kv, _i32p), kv.size, nf, int(g["k_fold"]), ptr(lf, _i32p), 1,
+            int(g["auto_feature"]), 0)
+    assert rc == int(g["num_final"]), _lib.last_error()
+    mask = np.zeros(d, np.int32)
+    order = np.zeros(d, np.int32)
+    errs = np.zeros(d, np.float32)
+    L.get_selected_dimensions(ptr(mask, _i32p), d)
+    L.get_selected_ordering(ptr(order, _i32p), d)
+    L.get_selected_errors(ptr(errs, _f32p), d)
+    np.testing.assert_array_equal(order, g["ordering"])
+    np.testing.assert_array_equal(mask, g["mask"])
+    np.testing.assert_array_equal(errs, g["errors"])
+    assert L.get_final_optimal_model_k() == int(g["best_k"])
+
+
+@pytest.mark.parametrize("name", NN_CASES)
+def test_neighbour_lists_match_reference(name):
+    g = _g(name)
+    committed = list(g["committed"])
+    method = str(g["method"])
+    kmax = int(g["k_max"])
+    X, y = g["X"], g["y"]
+    p = X.shape[1]
+    # drive the selector to the committed state, then score once with lists kept
+    with Selector(X, y, k_vals=[kmax], num_features=p if method == "forward" else 0, method=method,
+                  k_fold=int(g["k_fold"])) as s:
+        s.commit_sequence(committed)
+        s.keep_neighbours(True)
+        assert s.step()
+        cands, idx, dist = s.neighbours()
+    want = list(g["candidates"])
+    for ci, c in enumerate(want):
+        j = list(cands).index(c)
+        np.testing.assert_array_equal(idx[j], g["nn_idx"][ci])
+        np.testing.assert_array_equal(dist[j], g["nn_dist"][ci])
+
+
+def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, **kw):
+    s = datagen.generate(n_train, n_val, p, n_mag=kw.pop("n_mag", 5), seed=seed, **kw)
+    prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
+    o = oracle.select(prob, k_vals, nf, method)
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=k_vals, num_features=nf, method=method) as sel:
+        r = sel.run()
+    return o, r
+
+
+@pytest.mark.parametrize("args", [
+    (2000, 1000, 20, 0, [10], 8, "forward"),          # the CPU-size forward workload
+    (1500, 700, 16, 7, [1, 4, 9], 5, "forward"),
+    (1200, 601, 18, 8, [5], 12, "backward"),
+    (999, 333, 12, 9, [3, 30], 4, "forward"),          # k_max 30 -> 4 candidates per thread
+    (700, 257, 10, 10, [64], 3, "forward"),            # k_max 64 -> 2 per thread
+    (400, 130, 9, 11, [150, 2], 2, "backward"),        # k_max 150 -> 1 per thread
+])
+def test_holdout_matches_oracle(args):
+    n_train, n_val, p, seed, kv, nf, method = args
+    o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method)
+    np.testing.assert_array_equal(r["ordering"], o["ordering"])
+    np.testing.assert_array_equal(r["mask"], o["mask"])
+    np.testing.assert_array_equal(r["errors"], o["errors"])
+    np.testing.assert_array_equal(r["step_best_k"], o["step_best_k"])
+    np.testing.assert_allclose(r["errors64"], o["errors64"], rtol=ERR64_RTOL, atol=0)
+    assert r["best_k"] == o["best_k"] and r["num_final"] == o["num_final"]
+
+
+def test_holdout_neighbours_match_oracle():
+    s = datagen.generate(3000, 1100, 24, n_mag=6, n_heavy=4, seed=21)
+    kv = [7, 2]
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=kv, num_features=4, method="forward") as sel:
+        for _ in range(2):
+            assert sel.step()
+        committed = list(sel.results()["ordering"][:2])
+        sel.keep_neighbours(True)
+        assert sel.step()
+        cands, idx, dist = sel.neighbours()
+    prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
+    o = oracle.step(prob, kv, committed, list(cands))
+    np.testing.assert_array_equal(idx, o["nn_idx"])
+    np.testing.assert_array_equal(dist, o["nn_dist"])
+
+
+def test_duplicate_training_rows_tie_rule():
+    """2 % duplicated training rows (exact distance ties) on the mixture generator."""
+    s = datagen.generate(2500, 800, 14, n_mag=6, seed=31, mixture=True, dup_frac=0.02)
+    o, r = None, None
+    prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
+    o = oracle.select(prob, [5, 50], 5, "forward")
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=[5, 50], num_features=5, method="forward") as sel:
+        r = sel.run()
+    np.testing.assert_array_equal(r["ordering"], o["ordering"])
+    np.testing.assert_array_equal(r["errors"], o["errors"])
+
+
+def test_step_api_equals_run_and_is_deterministic():
+    s = datagen.generate(4096, 2048, 30, n_mag=8, n_heavy=5, seed=41)
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=[10], num_features=6, method="forward") as sel:
+        a = sel.run()
+        b = sel.run()
+        sel.reset()
+        n = 0
+        while sel.step():
+            n += 1
+        c = sel.results()
+    assert n == 6
+    for k in ("ordering", "mask", "errors", "errors64", "step_best_k"):
+        np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_array_equal(a[k], c[k])
+
+
+def test_nan_labels_report_no_winner():
+    s = datagen.generate(300, 100, 6, n_mag=5, seed=51)
+    yv = s.yval.copy()
+    yv[:] = np.nan
+    with Selector(s.Xtrain, s.ytrain, s.Xval, yv, k_vals=[3], num_features=2) as sel:
+        with pytest.raises(_lib.SnnError) as e:
+            sel.run()
+    assert e.value.code == _lib.SNN_ERR_NO_WINNER
+
+
+def test_headline_shape_subset_rows_against_oracle():
+    """The 64k x 32k x 60 forward workload at a reduced row count: neighbour
+    lists and errors against the oracle for the first two steps."""
+    s = datagen.generate(16384, 1024, 60, n_mag=8, n_heavy=10, seed=2)
+    kv = [10]
+    prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=kv, num_features=3, method="forward") as sel:
+        sel.keep_neighbours(True)
+        assert sel.step()
+        cands, idx, dist = sel.neighbours()
+        r = sel.results()
+    o = oracle.step(prob, kv, [], list(cands))
+    np.testing.assert_array_equal(idx, o["nn_idx"])
+    errs = np.array([oracle.rmse32(o["sq32"][ci, 0]) for ci in range(len(cands))])
+    w = int(np.argmin(errs))
+    assert r["ordering"][0] == cands[w]
+    assert r["errors"][0] == errs[w]
