@@ -276,6 +276,9 @@ def run_ours(args, world, rank, local):
     w = dict(datagen.WORKLOADS[WORKLOAD])
     k, steps = w.pop("k"), w.pop("select")
     w["seed"] = w["seed"] + 1000 * rank
+    if args.rows_scale != 1.0:
+        w["n_train"] = int(w["n_train"] * args.rows_scale)
+        w["n_val"] = int(w["n_val"] * args.rows_scale)
     split = datagen.generate(**w)
     n_train, n_val, p = split.Xtrain.shape[0], split.Xval.shape[0], split.Xtrain.shape[1]
     evals = cand_evals(n_val, n_train, p, steps)
@@ -324,7 +327,7 @@ def run_ours(args, world, rank, local):
     barrier()
     e0 = time.perf_counter()
     d2h = 0
-    for _ in range(args.steps):
+    for _ in range(0 if args.no_e2e else args.steps):
         _lib.check(L.snn_load(sel._h, ptr(hx, _f32p), ptr(hy, _f32p), ptr(hxv, _f32p), ptr(hyv, _f32p)))
         _lib.check(L.snn_run(sel._h))
         r = sel.results()
@@ -358,8 +361,8 @@ def run_ours(args, world, rank, local):
             "breakdown_ms_per_step": {"score": score_ms / args.steps, "commit": commit_ms / args.steps,
                                       "other": (tot_ms - score_ms - commit_ms) / args.steps},
             "wall_ms_per_step": 1000.0 * wall / args.steps,
-            "e2e": {"value": world * evals / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+            "e2e": None if args.no_e2e else {"value": world * evals / e2e_s, "unit": UNIT,
+                                             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
             "roofline": {"bound": "fp32", "kernel": "k_score", "achieved": achieved_fp32, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved_fp32 / fp32_peak,
@@ -398,6 +401,9 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=64, help="validation rows per process per reference step")
     ap.add_argument("--cpu-rows", type=int, default=96, help="validation rows per process for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows-scale", type=float, default=1.0,
+                    help="scale n_train and n_val (small cases for profiler captures; not the bench workload)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiler captures)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per scoring launch, scaled to this workload (reported as roofline.traffic)")
     args = ap.parse_args()

@@ -163,7 +163,7 @@ def test_step_api_equals_run_and_is_deterministic():
 
 
 def test_nan_labels_report_no_winner():
-    s = datagen.generate(300, 100, 6, n_mag=5, seed=51)
+    s = datagen.generate(300, 100, 9, n_mag=5, seed=51)
     yv = s.yval.copy()
     yv[:] = np.nan
     with Selector(s.Xtrain, s.ytrain, s.Xval, yv, k_vals=[3], num_features=2) as sel:
