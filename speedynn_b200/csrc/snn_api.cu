@@ -60,7 +60,7 @@ struct snn_handle {
     int n_rows = 0, n_cols = 0, p = 0, cv = 0, npf = 1, kmax = 0, nk = 0;
     int ldc = 0, ldr = 0;
     int total_steps = 0;
-    int cc = 0;
+    snn::ScorePlan plan{0, 0, 0};
     int device = 0;
     cudaStream_t stream = nullptr;
     // device buffers
@@ -185,7 +185,7 @@ int issue_step(snn_handle *h, int t)
     EventPair &se = h->score_ev[h->n_score];
     if (int rc = make_pair(se)) return rc;
     SNN_CUDA(cudaEventRecord(se.a, h->stream));
-    SNN_CUDA(snn::launch_score(b, n_cand, h->cc, backward, h->stream));
+    SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
     SNN_CUDA(cudaEventRecord(se.b, h->stream));
     h->n_score++;
     SNN_CUDA(snn::launch_reduce(b, n_cand, h->stream));
@@ -289,8 +289,9 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (cudaSetDevice(h->device) != cudaSuccess) return bail(fail(SNN_ERR_CUDA, "cudaSetDevice(%d) failed", h->device));
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-    h->cc = snn::pick_score_cc(kmax, max_smem);
-    if (h->cc == 0) return bail(fail(SNN_ERR_UNSUPPORTED, "k_max=%d needs more shared memory than a block has", kmax));
+    h->plan = snn::plan_score(kmax, d->p, max_smem);
+    if (h->plan.cc == 0)
+        return bail(fail(SNN_ERR_UNSUPPORTED, "k_max=%d is above the supported maximum of %d", kmax, snn::kScoreMaxK));
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(SNN_ERR_CUDA, "cudaStreamCreate failed"));
 

@@ -54,17 +54,22 @@ struct Bufs {
     float *nn_dist;
 };
 
-constexpr int kScoreRows = 128;  // rows (threads) per scoring block
-constexpr int kTileCols = 32;    // columns per D tile
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D
+constexpr int kScoreMaxK = 256;  // largest k_max of the scoring kernel
 
-size_t score_smem_bytes(int cc, int kmax);
-int pick_score_cc(int kmax, int max_smem);
+// Launch shape of the scoring kernel: cc candidates per thread, `warps`
+// warps per block (32 scored rows per block), dynamic shared memory bytes.
+struct ScorePlan {
+    int cc;
+    int warps;
+    int smem;
+};
+ScorePlan plan_score(int kmax, int p, int max_smem);
 
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);
 cudaError_t launch_init_forward(const Bufs &b, int cv, int npf, cudaStream_t s);
 cudaError_t launch_full_distance(const Bufs &b, int cv, int npf, cudaStream_t s);
-cudaError_t launch_score(const Bufs &b, int n_cand, int cc, int backward, cudaStream_t s);
+cudaError_t launch_score(const Bufs &b, int n_cand, const ScorePlan &plan, int backward, cudaStream_t s);
 cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s);
 cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_steps, int backward,
                           int auto_feature, cudaStream_t s);

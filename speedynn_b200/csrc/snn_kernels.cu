@@ -137,161 +137,6 @@ __global__ void __launch_bounds__(256) k_full_distance(Bufs b, int cv, int npf)
 }
 
 // ---------------------------------------------------------------------------
-// Candidate scoring (the hot kernel).
-//
-// One thread owns one scored row r and CC candidate features; a block owns
-// 128 rows and one chunk of CC candidates and streams the row block of D
-// through shared memory in 32-column tiles (coalesced float4 loads, register
-// prefetch of the next tile, stored transposed so each thread reads its own
-// row conflict-free).  The candidate columns of X for the tile sit in shared
-// memory and are read as broadcasts; x_r,c lives in registers.  Each
-// (row, candidate) keeps its top-k_max list in shared memory, interleaved by
-// thread, with the k-th distance cached in a register as the entry test.
-// The epilogue forms the kNN-mean predictions for every k of k_vals.
-// ---------------------------------------------------------------------------
-constexpr int kDsLd = kScoreRows + 1;
-
-__device__ __forceinline__ float list_insert(float *Ld, int *Li, int base, int K, float d, int i)
-{
-    int pos = K - 1;
-    while (pos > 0) {
-        const float prev = Ld[base + (pos - 1) * kScoreRows];
-        if (!(prev > d)) break;
-        Ld[base + pos * kScoreRows] = prev;
-        Li[base + pos * kScoreRows] = Li[base + (pos - 1) * kScoreRows];
-        --pos;
-    }
-    Ld[base + pos * kScoreRows] = d;
-    Li[base + pos * kScoreRows] = i;
-    return Ld[base + (K - 1) * kScoreRows];
-}
-
-template <int CC, bool BWD>
-__global__ void __launch_bounds__(kScoreRows) k_score(Bufs b, int n_cand, int n_chunks)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *Ds = reinterpret_cast<float *>(smem_raw);           // [kTileCols][kDsLd]
-    float *Xs = Ds + kTileCols * kDsLd;                          // [kTileCols][CC]
-    int *scand = reinterpret_cast<int *>(Xs + kTileCols * CC);   // [CC]
-    float *Ld = reinterpret_cast<float *>(scand + CC);           // [CC][K][kScoreRows]
-    const int K = b.kmax;
-    int *Li = reinterpret_cast<int *>(Ld + (size_t)CC * K * kScoreRows);
-
-    if (b.st->done) return;
-
-    const int tid = threadIdx.x;
-    const int chunk = blockIdx.x % n_chunks;
-    const int r0 = (blockIdx.x / n_chunks) * kScoreRows;
-    const int r = r0 + tid;
-    const bool rvalid = r < b.n_rows;
-    const int c0 = chunk * CC;
-
-    if (tid < CC) {
-        const int ci = c0 + tid;
-        scand[tid] = b.cands[ci < n_cand ? ci : 0];
-    }
-    __syncthreads();
-
-    float xv[CC], thr[CC];
-#pragma unroll
-    for (int c = 0; c < CC; ++c) {
-        xv[c] = rvalid ? b.XV[(size_t)scand[c] * b.ldr + r] : 0.0f;
-        thr[c] = FLT_MAX;
-    }
-    for (int c = 0; c < CC; ++c)
-        for (int j = 0; j < K; ++j) {
-            Ld[(c * K + j) * kScoreRows + tid] = FLT_MAX;
-            Li[(c * K + j) * kScoreRows + tid] = 0;
-        }
-
-    // tile loaders: 128 rows x 32 cols of D = 1024 float4, 8 per thread;
-    // CC x 32 candidate values = CC*8 float4.
-    float4 dreg[8];
-    float4 xreg = make_float4(0.f, 0.f, 0.f, 0.f);
-    auto load_tile = [&](int tile) {
-        const int i0 = tile * kTileCols;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int f = tid + kScoreRows * q;
-            const int row = f >> 3, c4 = f & 7;
-            if (r0 + row < b.n_rows)
-                dreg[q] = __ldcs(reinterpret_cast<const float4 *>(b.D + (size_t)(r0 + row) * b.ldc + i0 + c4 * 4));
-            else
-                dreg[q] = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
-        }
-        if (tid < CC * 8) {
-            const int c = tid >> 3, c4 = tid & 7;
-            xreg = __ldg(reinterpret_cast<const float4 *>(b.XT + (size_t)scand[c] * b.ldc + i0 + c4 * 4));
-        }
-    };
-    auto store_tile = [&]() {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int f = tid + kScoreRows * q;
-            const int row = f >> 3, c4 = f & 7;
-            Ds[(c4 * 4 + 0) * kDsLd + row] = dreg[q].x;
-            Ds[(c4 * 4 + 1) * kDsLd + row] = dreg[q].y;
-            Ds[(c4 * 4 + 2) * kDsLd + row] = dreg[q].z;
-            Ds[(c4 * 4 + 3) * kDsLd + row] = dreg[q].w;
-        }
-        if (tid < CC * 8) {
-            const int c = tid >> 3, c4 = tid & 7;
-            Xs[(c4 * 4 + 0) * CC + c] = xreg.x;
-            Xs[(c4 * 4 + 1) * CC + c] = xreg.y;
-            Xs[(c4 * 4 + 2) * CC + c] = xreg.z;
-            Xs[(c4 * 4 + 3) * CC + c] = xreg.w;
-        }
-    };
-
-    const int ntiles = b.ldc / kTileCols;
-    load_tile(0);
-    for (int tile = 0; tile < ntiles; ++tile) {
-        __syncthreads();
-        store_tile();
-        __syncthreads();
-        if (tile + 1 < ntiles) load_tile(tile + 1);
-        if (rvalid) {
-            const int i0 = tile * kTileCols;
-#pragma unroll 2
-            for (int j = 0; j < kTileCols; ++j) {
-                const float dv = Ds[j * kDsLd + tid];
-#pragma unroll
-                for (int c = 0; c < CC; ++c) {
-                    const float s = sqdiff(xv[c], Xs[j * CC + c]);
-                    const float d = BWD ? __fsub_rn(dv, s) : __fadd_rn(dv, s);
-                    if (d < thr[c]) thr[c] = list_insert(Ld, Li, c * K * kScoreRows + tid, K, d, i0 + j);
-                }
-            }
-        }
-    }
-
-    if (!rvalid) return;
-#pragma unroll
-    for (int c = 0; c < CC; ++c) {
-        const int slot = c0 + c;
-        if (slot >= n_cand) continue;
-        const int base = c * K * kScoreRows + tid;
-        if (b.nn_idx) {
-            const size_t o = ((size_t)slot * b.n_rows + r) * K;
-            for (int j = 0; j < K; ++j) {
-                b.nn_idx[o + j] = Li[base + j * kScoreRows];
-                b.nn_dist[o + j] = Ld[base + j * kScoreRows];
-            }
-        }
-        // label prefix sums in rank order, in place of the distances
-        float acc = 0.0f;
-        for (int j = 0; j < K; ++j) {
-            acc = __fadd_rn(acc, __ldg(b.yc + Li[base + j * kScoreRows]));
-            Ld[base + j * kScoreRows] = acc;
-        }
-        for (int m = 0; m < b.nk; ++m) {
-            const int k = __ldg(b.kvals + m);
-            b.pred[((size_t)slot * b.nk + m) * b.n_rows + r] = __fdiv_rn(Ld[base + (k - 1) * kScoreRows], (float)k);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Per (candidate, k) error: one warp per pair.  Lanes form the squared
 // residuals in parallel; lane 0 adds them in row order in FP32 (the
 // reference's sequential sum); every lane also accumulates its residuals in
@@ -497,20 +342,6 @@ int sm_count()
 
 }  // namespace
 
-size_t score_smem_bytes(int cc, int kmax)
-{
-    return sizeof(float) * (size_t)kTileCols * kDsLd + sizeof(float) * (size_t)kTileCols * cc + sizeof(int) * (size_t)cc +
-           (sizeof(float) + sizeof(int)) * (size_t)cc * kmax * kScoreRows;
-}
-
-int pick_score_cc(int kmax, int max_smem)
-{
-    const int ccs[4] = {8, 4, 2, 1};
-    for (int i = 0; i < 4; ++i)
-        if (score_smem_bytes(ccs[i], kmax) <= (size_t)max_smem) return ccs[i];
-    return 0;
-}
-
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s)
 {
     dim3 grid((ld + 31) / 32, (p + 31) / 32);
@@ -530,35 +361,6 @@ cudaError_t launch_full_distance(const Bufs &b, int cv, int npf, cudaStream_t s)
     dim3 grid(b.ldc / kFdTile, (b.n_rows + kFdTile - 1) / kFdTile);
     k_full_distance<<<grid, 256, 0, s>>>(b, cv, npf);
     return cudaGetLastError();
-}
-
-template <int CC>
-static cudaError_t launch_score_cc(const Bufs &b, int n_cand, int backward, cudaStream_t s)
-{
-    const int n_chunks = (n_cand + CC - 1) / CC;
-    const int n_rb = (b.n_rows + kScoreRows - 1) / kScoreRows;
-    const size_t smem = score_smem_bytes(CC, b.kmax);
-    const long long blocks = (long long)n_chunks * n_rb;
-    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    if (backward) {
-        cudaFuncSetAttribute(k_score<CC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_score<CC, true><<<(unsigned)blocks, kScoreRows, smem, s>>>(b, n_cand, n_chunks);
-    } else {
-        cudaFuncSetAttribute(k_score<CC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_score<CC, false><<<(unsigned)blocks, kScoreRows, smem, s>>>(b, n_cand, n_chunks);
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_score(const Bufs &b, int n_cand, int cc, int backward, cudaStream_t s)
-{
-    switch (cc) {
-    case 8: return launch_score_cc<8>(b, n_cand, backward, s);
-    case 4: return launch_score_cc<4>(b, n_cand, backward, s);
-    case 2: return launch_score_cc<2>(b, n_cand, backward, s);
-    case 1: return launch_score_cc<1>(b, n_cand, backward, s);
-    default: return cudaErrorInvalidValue;
-    }
 }
 
 cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s)
