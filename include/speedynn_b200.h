@@ -155,6 +155,18 @@ SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_ma
 SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches, double *commit_ms,
                            int *commit_launches, double *total_ms, int *total_launches);
 
+/* Options (all default on):
+ *   SNN_OPT_PRUNE  forward steps after the first skip training columns whose
+ *                  committed distance already exceeds every candidate's bound
+ *                  on its k-th neighbour distance (exact: same results);
+ *                  0 forces the full scan of every column. */
+#define SNN_OPT_PRUNE 1
+SNN_API int snn_set_option(snn_handle *h, int option, int value);
+
+/* Work counters since the last run/step/reset: (row, column) pairs the pruned
+ * scorer streamed, and how many of them it had to score. */
+SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, unsigned long long *pairs_survived);
+
 SNN_API int snn_destroy(snn_handle *h);
 
 /* Message of the last failure on the calling thread ("" if none). */

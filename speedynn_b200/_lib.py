@@ -18,6 +18,8 @@ SNN_ERR_UNSUPPORTED = -4
 SNN_ERR_NO_WINNER = -5
 SNN_ERR_STATE = -6
 
+SNN_OPT_PRUNE = 1
+
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f32p = ctypes.POINTER(ctypes.c_float)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -67,6 +69,8 @@ def lib():
             "snn_get_neighbours": (ctypes.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _f32p]),
             "snn_get_timing": (ctypes.c_int, [vp, _f64p, _i32p, _f64p, _i32p, _f64p, _i32p]),
             "snn_destroy": (ctypes.c_int, [vp]),
+            "snn_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+            "snn_get_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]),
             "snn_last_error": (ctypes.c_char_p, []),
             "snn_version": (ctypes.c_char_p, []),
             "train_forward_selection": (ctypes.c_int, [_f32p, ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int, _i32p,

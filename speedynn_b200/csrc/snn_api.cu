@@ -69,6 +69,14 @@ struct snn_handle {
     double *rmse64 = nullptr, *err64 = nullptr;
     int *kv = nullptr, *cands = nullptr, *prev_cands = nullptr, *mask = nullptr, *order = nullptr, *stepk = nullptr;
     State *st = nullptr;
+    // pruned forward path
+    float *Xrow = nullptr;        // training points, row-major
+    int *seeds = nullptr;         // [n_rows][M]
+    int M = 0;
+    unsigned long long *survivors = nullptr;
+    bool prune = true;
+    int max_smem = 0;
+    unsigned long long scanned_pairs = 0;  // host count of (row, column) pairs the pruned path streamed
     int *nn_idx = nullptr;
     float *nn_dist = nullptr;
     bool keep_nn = false;
@@ -135,7 +143,7 @@ void free_all(snn_handle *h)
     cudaSetDevice(h->device);
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                    h->stepk, h->st, h->nn_idx, h->nn_dist};
+                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : h->score_ev) {
@@ -174,6 +182,14 @@ int check_device(int device)
     return SNN_OK;
 }
 
+// The pruned scorer needs the seed columns written by the previous forward
+// commit, a k small enough for them, and shared memory for the lists.
+bool use_sparse(const snn_handle *h, int t, int n_cand)
+{
+    return h->prune && !h->desc.backward && t >= 1 && h->M > 0 && n_cand <= 128 &&
+           snn::sparse_smem_per_warp(n_cand, h->kmax) <= (size_t)h->max_smem;
+}
+
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)
 {
@@ -185,7 +201,13 @@ int issue_step(snn_handle *h, int t)
     EventPair &se = h->score_ev[h->n_score];
     if (int rc = make_pair(se)) return rc;
     SNN_CUDA(cudaEventRecord(se.a, h->stream));
-    SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
+    if (use_sparse(h, t, n_cand)) {
+        snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
+        SNN_CUDA(snn::launch_score_sparse(b, sp, n_cand, h->M, h->max_smem, h->stream));
+        h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
+    } else {
+        SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
+    }
     SNN_CUDA(cudaEventRecord(se.b, h->stream));
     h->n_score++;
     SNN_CUDA(snn::launch_reduce(b, n_cand, h->stream));
@@ -197,7 +219,7 @@ int issue_step(snn_handle *h, int t)
         EventPair &ce = h->commit_ev[h->n_commit];
         if (int rc = make_pair(ce)) return rc;
         SNN_CUDA(cudaEventRecord(ce.a, h->stream));
-        SNN_CUDA(snn::launch_commit(b, backward, h->stream));
+        SNN_CUDA(snn::launch_commit_seeds(b, backward, backward ? nullptr : h->seeds, h->M, h->stream));
         SNN_CUDA(cudaEventRecord(ce.b, h->stream));
         h->n_commit++;
         h->n_launch += 1;
@@ -228,6 +250,8 @@ int read_state(snn_handle *h, State *s)
 void reset_timing(snn_handle *h)
 {
     h->n_score = h->n_commit = h->n_launch = 0;
+    h->scanned_pairs = 0;
+    if (h->survivors) cudaMemsetAsync(h->survivors, 0, sizeof(unsigned long long), h->stream);
 }
 
 }  // namespace
@@ -289,6 +313,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (cudaSetDevice(h->device) != cudaSuccess) return bail(fail(SNN_ERR_CUDA, "cudaSetDevice(%d) failed", h->device));
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    h->max_smem = max_smem;
     h->plan = snn::plan_score(kmax, d->p, max_smem);
     if (h->plan.cc == 0)
         return bail(fail(SNN_ERR_UNSUPPORTED, "k_max=%d is above the supported maximum of %d", kmax, snn::kScoreMaxK));
@@ -318,6 +343,10 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->order, p, "ordering"))) return bail(rc);
     if ((rc = dev_alloc(&h->stepk, p, "best k"))) return bail(rc);
     if ((rc = dev_alloc(&h->st, 1, "state"))) return bail(rc);
+    if ((rc = dev_alloc(&h->Xrow, p * h->n_cols, "X_train rows"))) return bail(rc);
+    if ((rc = dev_alloc(&h->survivors, 1, "counters"))) return bail(rc);
+    h->M = d->backward ? 0 : snn::seeds_for_k(kmax);
+    if (h->M > 0 && (rc = dev_alloc(&h->seeds, (size_t)h->n_rows * h->M, "seed columns"))) return bail(rc);
     if (cudaMemcpy(h->kv, h->kvals.data(), sizeof(int) * h->nk, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(SNN_ERR_CUDA, "copy of k_vals failed"));
     if (make_pair(h->total_ev)) return bail(SNN_ERR_CUDA);
@@ -351,6 +380,8 @@ static int load_impl(snn_handle *h, const float *X_train, const float *y_train, 
     SNN_CUDA(cudaSetDevice(h->device));
     const cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (int rc = load_matrix(h, X_train, h->n_cols, h->XT, h->ldc, device_src)) return rc;
+    SNN_CUDA(cudaMemcpyAsync(h->Xrow, device_src ? X_train : h->stage, sizeof(float) * (size_t)h->n_cols * h->p,
+                             cudaMemcpyDeviceToDevice, h->stream));
     SNN_CUDA(cudaMemcpyAsync(h->yc, y_train, sizeof(float) * h->n_cols, kind, h->stream));
     if (!h->cv) {
         // the staging buffer is reused: order the second upload after the first transpose
@@ -441,7 +472,7 @@ SNN_API int snn_commit_sequence(snn_handle *h, const int *seq, int n)
     for (int t = 0; t < n; ++t) {
         const int it = h->desc.backward ? h->p - 1 - t : t;
         SNN_CUDA(snn::launch_force(b, seq[t], it, t, h->total_steps, h->desc.backward, h->stream));
-        SNN_CUDA(snn::launch_commit(b, h->desc.backward, h->stream));
+        SNN_CUDA(snn::launch_commit_seeds(b, h->desc.backward, h->desc.backward ? nullptr : h->seeds, h->M, h->stream));
     }
     h->host_step = n;
     SNN_CUDA(cudaStreamSynchronize(h->stream));
@@ -530,6 +561,29 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
     if (commit_launches) *commit_launches = h->n_commit;
     if (total_ms) *total_ms = tot;
     if (total_launches) *total_launches = h->n_launch;
+    return SNN_OK;
+}
+
+SNN_API int snn_set_option(snn_handle *h, int option, int value)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    switch (option) {
+    case SNN_OPT_PRUNE: h->prune = value != 0; return SNN_OK;
+    default: return fail(SNN_ERR_ARG, "unknown option %d", option);
+    }
+}
+
+SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, unsigned long long *pairs_survived)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    SNN_CUDA(cudaSetDevice(h->device));
+    unsigned long long sv = 0;
+    SNN_CUDA(cudaMemcpyAsync(&sv, h->survivors, sizeof sv, cudaMemcpyDeviceToHost, h->stream));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    if (pairs_streamed) *pairs_streamed = h->scanned_pairs;
+    if (pairs_survived) *pairs_survived = sv;
     return SNN_OK;
 }
 

@@ -66,6 +66,19 @@ struct ScorePlan {
 };
 ScorePlan plan_score(int kmax, int p, int max_smem);
 
+// Pruned forward scoring (snn_sparse.cu).
+constexpr int kMaxSeeds = 128;  // seed columns per row (multiple of 32)
+struct SparseBufs {
+    const float *Xrow;                  // training points, row-major [n_cols][ldp]
+    int ldp;
+    int *seeds;                         // [n_rows][M] nearest columns under the committed D
+    unsigned long long *survivors;      // optional counter of scanned-in columns
+};
+size_t sparse_smem_per_warp(int n_cand, int kmax);
+int seeds_for_k(int kmax);  // 0: k too large for the pruned path
+cudaError_t launch_commit_seeds(const Bufs &b, int backward, int *seeds, int M, cudaStream_t s);
+cudaError_t launch_score_sparse(const Bufs &b, const SparseBufs &sp, int n_cand, int M, int max_smem, cudaStream_t s);
+
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);
 cudaError_t launch_init_forward(const Bufs &b, int cv, int npf, cudaStream_t s);
 cudaError_t launch_full_distance(const Bufs &b, int cv, int npf, cudaStream_t s);
@@ -73,7 +86,6 @@ cudaError_t launch_score(const Bufs &b, int n_cand, const ScorePlan &plan, int b
 cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s);
 cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_steps, int backward,
                           int auto_feature, cudaStream_t s);
-cudaError_t launch_commit(const Bufs &b, int backward, cudaStream_t s);
 cudaError_t launch_reset_state(const Bufs &b, int backward, int total_steps, cudaStream_t s);
 cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s);
 

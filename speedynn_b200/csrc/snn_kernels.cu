@@ -246,41 +246,6 @@ __global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int
     if (t + 1 >= total_steps) st->done = 1;
 }
 
-// ---------------------------------------------------------------------------
-// Commit the winner into D in place: D = fl(D +/- fl(fl(x_r,w - x_i,w)^2))
-// (speedynn/lib/cpu.c:301-315).  HBM-bound: one read + one write per entry.
-// Excluded / pad entries stay +inf.
-// ---------------------------------------------------------------------------
-template <bool BWD>
-__global__ void __launch_bounds__(256) k_commit(Bufs b)
-{
-    if (b.st->done) return;
-    const int w = b.st->winner;
-    const float *xt = b.XT + (size_t)w * b.ldc;
-    const float *xv = b.XV + (size_t)w * b.ldr;
-    const int ld4 = b.ldc >> 2;
-    for (int r = blockIdx.x; r < b.n_rows; r += gridDim.x) {
-        const float a = __ldg(xv + r);
-        float4 *row = reinterpret_cast<float4 *>(b.D + (size_t)r * b.ldc);
-        for (int q = threadIdx.x; q < ld4; q += blockDim.x) {
-            const float4 c = __ldg(reinterpret_cast<const float4 *>(xt) + q);
-            float4 d = __ldcs(row + q);
-            if (BWD) {
-                d.x = __fsub_rn(d.x, sqdiff(a, c.x));
-                d.y = __fsub_rn(d.y, sqdiff(a, c.y));
-                d.z = __fsub_rn(d.z, sqdiff(a, c.z));
-                d.w = __fsub_rn(d.w, sqdiff(a, c.w));
-            } else {
-                d.x = __fadd_rn(d.x, sqdiff(a, c.x));
-                d.y = __fadd_rn(d.y, sqdiff(a, c.y));
-                d.z = __fadd_rn(d.z, sqdiff(a, c.z));
-                d.w = __fadd_rn(d.w, sqdiff(a, c.w));
-            }
-            __stcs(row + q, d);
-        }
-    }
-}
-
 // Warm start: record a given winner without scoring (same bookkeeping as
 // k_select), so the commit kernel and later steps see it.
 __global__ void k_force(Bufs b, int w, int it, int t, int total_steps, int backward)
@@ -374,16 +339,6 @@ cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_st
                           cudaStream_t s)
 {
     k_select<<<1, 32, 0, s>>>(b, n_cand, it, t, total_steps, backward, auto_feature);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_commit(const Bufs &b, int backward, cudaStream_t s)
-{
-    int grid = b.n_rows < sm_count() * 8 ? b.n_rows : sm_count() * 8;
-    if (backward)
-        k_commit<true><<<grid, 256, 0, s>>>(b);
-    else
-        k_commit<false><<<grid, 256, 0, s>>>(b);
     return cudaGetLastError();
 }
 

@@ -13,8 +13,13 @@
 //     candidates' 32-column slices of X stream through a 3-stage cp.async
 //     ring, so each D element leaves L2 once per block and every warp reuses it;
 //   * arithmetic pairs two adjacent columns of one candidate in packed FP32
-//     (sub/mul/add.rn.f32x2: explicit rounding, never contracted to FMA), so a
-//     pair of evaluations costs three issue slots plus two compares;
+//     (sub/fma/add.rn.f32x2), so a pair of evaluations costs three issue
+//     slots plus two compares.  The square is formed as fma.rn.f32x2(t, t, +0)
+//     rather than mul.rn.f32x2: ptxas contracts a single-use packed
+//     mul.rn + add.rn pair into one FMA despite the rounding modifiers (about
+//     17 % of results then differ by one ulp from the reference's two
+//     roundings), while fl(t*t + 0) = fl(t*t) for t*t >= 0 and cannot be
+//     folded into the following add;
 //   * each (row, candidate) keeps its current k-th distance in a register;
 //     four columns are tested against it and one warp vote decides whether
 //     anything must be inserted;
@@ -35,7 +40,6 @@ constexpr int kRows = 32;           // scored rows per block (one per lane)
 constexpr int kCols = 32;           // columns per tile
 constexpr int kDsLd = kCols + 4;    // padded row stride of the D tile (conflict-free 128-bit reads)
 constexpr int kStages = 3;          // cp.async ring depth
-constexpr int kGMax = kScoreMaxK / 32;
 constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ unsigned long long as_u64(float2 v) { return *reinterpret_cast<unsigned long long *>(&v); }
@@ -53,10 +57,13 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b)
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
     return as_f2(d);
 }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+// fl(t*t), exactly as a rounded multiply, but immune to contraction with the
+// next add (see the file comment).
+__device__ __forceinline__ float2 sq2(float2 t)
 {
     unsigned long long d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
+    const unsigned long long z = 0ull;  // (+0.0f, +0.0f)
+    asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(d) : "l"(as_u64(t)), "l"(z));
     return as_f2(d);
 }
 
@@ -73,41 +80,38 @@ __device__ __forceinline__ void cp_async_wait()
 }
 
 // Insert (dv, col) into the sorted list at Ld/Li[base .. base+K) with all 32
-// lanes; the item goes after every element <= dv (stable: the scan visits
-// columns in ascending order).  Returns the new K-th distance.
-__device__ __forceinline__ float coop_insert(float *Ld, int *Li, int base, int K, int G, float dv, int col, int lane)
+// lanes (lane j holds elements j, j+32, ...); the item goes after every
+// element <= dv (stable: the scan visits columns in ascending order).
+// Returns the new K-th distance.  Kept out of line: it has many call sites
+// on the rare path and must not bloat the hot loop's instruction footprint.
+__device__ __noinline__ float coop_insert(float *Ld, int *Li, int base, int K, float dv, int col)
 {
-    float ev[kGMax];
-    int iv[kGMax];
+    const int lane = threadIdx.x & 31;
     int pos = 0;
-#pragma unroll
-    for (int g = 0; g < kGMax; ++g) {
-        if (g < G) {
-            const int x = g * 32 + lane;
-            const bool ok = x < K;
-            ev[g] = ok ? Ld[base + x] : FLT_MAX;
-            iv[g] = ok ? Li[base + x] : 0;
-            pos += __popc(__ballot_sync(kFull, ok && ev[g] <= dv));
-        }
+    for (int g0 = 0; g0 < K; g0 += 32) {
+        const int x = g0 + lane;
+        const bool ok = x < K;
+        const float e = ok ? Ld[base + x] : FLT_MAX;
+        pos += __popc(__ballot_sync(kFull, ok && e <= dv));
     }
     float carry_e = 0.0f;
     int carry_i = 0;
-#pragma unroll
-    for (int g = 0; g < kGMax; ++g) {
-        if (g < G) {
-            const int x = g * 32 + lane;
-            float up = __shfl_up_sync(kFull, ev[g], 1);
-            int upi = __shfl_up_sync(kFull, iv[g], 1);
-            if (lane == 0) {
-                up = carry_e;
-                upi = carry_i;
-            }
-            carry_e = __shfl_sync(kFull, ev[g], 31);
-            carry_i = __shfl_sync(kFull, iv[g], 31);
-            if (x < K && x >= pos) {
-                Ld[base + x] = (x == pos) ? dv : up;
-                Li[base + x] = (x == pos) ? col : upi;
-            }
+    for (int g0 = 0; g0 < K; g0 += 32) {
+        const int x = g0 + lane;
+        const bool ok = x < K;
+        const float e = ok ? Ld[base + x] : FLT_MAX;
+        const int ix = ok ? Li[base + x] : 0;
+        float up = __shfl_up_sync(kFull, e, 1);
+        int upi = __shfl_up_sync(kFull, ix, 1);
+        if (lane == 0) {
+            up = carry_e;
+            upi = carry_i;
+        }
+        carry_e = __shfl_sync(kFull, e, 31);
+        carry_i = __shfl_sync(kFull, ix, 31);
+        if (ok && x >= pos) {
+            Ld[base + x] = (x == pos) ? dv : up;
+            Li[base + x] = (x == pos) ? col : upi;
         }
     }
     __syncwarp();
@@ -138,7 +142,6 @@ __global__ void __launch_bounds__(512) k_score(Bufs b, int n_cand, int W, int n_
 {
     extern __shared__ __align__(16) float sm[];
     const int K = b.kmax;
-    const int G = (K + 31) >> 5;
     const int WCC = W * CC;
     const Layout S = carve(sm, WCC, K);
 
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(512) k_score(Bufs b, int n_cand, int W, int n_
                 const float4 xt = *reinterpret_cast<const float4 *>(Xw + c * kCols + q0);
                 const float2 t01 = sub2(xv2[c], make_float2(xt.x, xt.y));
                 const float2 t23 = sub2(xv2[c], make_float2(xt.z, xt.w));
-                const float2 s01 = mul2(t01, t01), s23 = mul2(t23, t23);
+                const float2 s01 = sq2(t01), s23 = sq2(t23);
                 e01[c] = BWD ? sub2(d01, s01) : add2(d01, s01);
                 e23[c] = BWD ? sub2(d23, s23) : add2(d23, s23);
                 pass |= (e01[c].x < thr[c]) | (e01[c].y < thr[c]) | (e23[c].x < thr[c]) | (e23[c].y < thr[c]);
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(512) k_score(Bufs b, int n_cand, int W, int n_
                             m &= m - 1;
                             const float dl = __shfl_sync(kFull, dq, L);
                             const int base = (L * WCC + w * CC + c) * K;
-                            const float nt = coop_insert(S.Ld, S.Li, base, K, G, dl, i0 + q0 + qq, lane);
+                            const float nt = coop_insert(S.Ld, S.Li, base, K, dl, i0 + q0 + qq);
                             if (lane == L) thr[c] = nt;
                         }
                     }

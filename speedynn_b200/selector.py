@@ -114,6 +114,15 @@ class Selector:
                                    ptr(dist, _f32p)))
         return cands, idx, dist
 
+    def set_pruning(self, enable):
+        """Exact pruning of forward steps after the first (on by default)."""
+        check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_PRUNE, int(bool(enable))))
+
+    def counters(self):
+        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        check(_lib.lib().snn_get_counters(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return {"pairs_streamed": a.value, "pairs_survived": b.value}
+
     def timing(self):
         s, c, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         ns, nc, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -189,3 +189,35 @@ def test_headline_shape_subset_rows_against_oracle():
     w = int(np.argmin(errs))
     assert r["ordering"][0] == cands[w]
     assert r["errors"][0] == errs[w]
+
+
+@pytest.mark.parametrize("args", [
+    (8192, 2048, 40, 61, [10], 8, dict(n_heavy=6)),
+    (6000, 1500, 24, 62, [5, 50], 6, dict(mixture=True, dup_frac=0.02)),
+    (3000, 0, 20, 63, [3, 7], 6, dict()),          # CV mode (n_val=0 -> rows are the training points)
+])
+def test_pruned_forward_equals_full_scan(args):
+    """Pruned forward steps (default) against the full scan of every column:
+    identical orderings, errors and neighbour lists, and the pruning prunes."""
+    n_train, n_val, p, seed, kv, nf, kw = args
+    s = datagen.generate(n_train, max(n_val, 1), p, n_mag=6, seed=seed, **kw)
+    Xv, yv = (s.Xval, s.yval) if n_val else (None, None)
+    out = {}
+    for prune in (True, False):
+        with Selector(s.Xtrain, s.ytrain, Xv, yv, k_vals=kv, num_features=nf, method="forward", k_fold=5) as sel:
+            sel.set_pruning(prune)
+            r = sel.run()
+            cnt = sel.counters()
+            sel.reset()
+            for _ in range(3):
+                sel.step()
+            sel.keep_neighbours(True)
+            sel.step()
+            out[prune] = (r, cnt, sel.neighbours())
+    (ra, ca, na), (rb, cb, nb) = out[True], out[False]
+    for k in ("ordering", "mask", "errors", "errors64", "step_best_k"):
+        np.testing.assert_array_equal(ra[k], rb[k])
+    for a, b in zip(na, nb):
+        np.testing.assert_array_equal(a, b)
+    assert ca["pairs_streamed"] > 0 and ca["pairs_survived"] < ca["pairs_streamed"]
+    assert cb["pairs_streamed"] == 0
