@@ -155,12 +155,17 @@ SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_ma
 SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches, double *commit_ms,
                            int *commit_launches, double *total_ms, int *total_launches);
 
-/* Options (all default on):
+/* Options:
  *   SNN_OPT_PRUNE  forward steps after the first skip training columns whose
  *                  committed distance already exceeds every candidate's bound
  *                  on its k-th neighbour distance (exact: same results);
  *                  0 forces the full scan of every column. */
 #define SNN_OPT_PRUNE 1
+/*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic (row per warp
+ *                  for k_max <= 64, else rows per lane), 1 rows per lane,
+ *                  2 row per warp.  Results are identical; this exists for
+ *                  cross-checks and measurement. */
+#define SNN_OPT_KERNEL 2
 SNN_API int snn_set_option(snn_handle *h, int option, int value);
 
 /* Work counters since the last run/step/reset: (row, column) pairs the pruned

@@ -19,6 +19,7 @@ SNN_ERR_NO_WINNER = -5
 SNN_ERR_STATE = -6
 
 SNN_OPT_PRUNE = 1
+SNN_OPT_KERNEL = 2
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f32p = ctypes.POINTER(ctypes.c_float)

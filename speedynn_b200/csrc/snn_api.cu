@@ -75,6 +75,7 @@ struct snn_handle {
     int M = 0;
     unsigned long long *survivors = nullptr;
     bool prune = true;
+    int kernel = 0;               // scoring kernel: 0 auto, 1 rows-per-lane, 2 row-per-warp
     int max_smem = 0;
     unsigned long long scanned_pairs = 0;  // host count of (row, column) pairs the pruned path streamed
     int *nn_idx = nullptr;
@@ -205,6 +206,8 @@ int issue_step(snn_handle *h, int t)
         snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
         SNN_CUDA(snn::launch_score_sparse(b, sp, n_cand, h->M, h->max_smem, h->stream));
         h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
+    } else if (h->kernel != 1 && snn::score_rw_supported(h->kmax)) {
+        SNN_CUDA(snn::launch_score_rw(b, n_cand, backward, h->stream));
     } else {
         SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
     }
@@ -570,6 +573,12 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value)
     if (!h) return fail(SNN_ERR_ARG, "null handle");
     switch (option) {
     case SNN_OPT_PRUNE: h->prune = value != 0; return SNN_OK;
+    case SNN_OPT_KERNEL:
+        if (value < 0 || value > 2) return fail(SNN_ERR_ARG, "kernel choice %d not in 0..2", value);
+        if (value == 2 && !snn::score_rw_supported(h->kmax))
+            return fail(SNN_ERR_UNSUPPORTED, "the row-per-warp kernel handles k_max <= 64");
+        h->kernel = value;
+        return SNN_OK;
     default: return fail(SNN_ERR_ARG, "unknown option %d", option);
     }
 }

@@ -66,6 +66,10 @@ struct ScorePlan {
 };
 ScorePlan plan_score(int kmax, int p, int max_smem);
 
+// Row-per-warp scoring (snn_score_rw.cu), k_max <= 64.
+bool score_rw_supported(int kmax);
+cudaError_t launch_score_rw(const Bufs &b, int n_cand, int backward, cudaStream_t s);
+
 // Pruned forward scoring (snn_sparse.cu).
 constexpr int kMaxSeeds = 128;  // seed columns per row (multiple of 32)
 struct SparseBufs {

@@ -118,6 +118,10 @@ class Selector:
         """Exact pruning of forward steps after the first (on by default)."""
         check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_PRUNE, int(bool(enable))))
 
+    def set_kernel(self, which):
+        """Full-scan scoring kernel: 0 automatic, 1 rows per lane, 2 row per warp."""
+        check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_KERNEL, int(which)))
+
     def counters(self):
         a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
         check(_lib.lib().snn_get_counters(self._h, ctypes.byref(a), ctypes.byref(b)))

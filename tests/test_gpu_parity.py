@@ -90,11 +90,12 @@ def test_neighbour_lists_match_reference(name):
         np.testing.assert_array_equal(dist[j], g["nn_dist"][ci])
 
 
-def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, **kw):
+def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, kernel=0, **kw):
     s = datagen.generate(n_train, n_val, p, n_mag=kw.pop("n_mag", 5), seed=seed, **kw)
     prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
     o = oracle.select(prob, k_vals, nf, method)
     with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=k_vals, num_features=nf, method=method) as sel:
+        sel.set_kernel(kernel)
         r = sel.run()
     return o, r
 
@@ -107,9 +108,12 @@ def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, **kw):
     (700, 257, 10, 10, [64], 3, "forward"),            # k_max 64 -> 2 per thread
     (400, 130, 9, 11, [150, 2], 2, "backward"),        # k_max 150 -> 1 per thread
 ])
-def test_holdout_matches_oracle(args):
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_holdout_matches_oracle(args, kernel):
     n_train, n_val, p, seed, kv, nf, method = args
-    o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method)
+    if kernel == 2 and max(kv) > 64:
+        pytest.skip("the row-per-warp kernel handles k_max <= 64")
+    o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method, kernel=kernel)
     np.testing.assert_array_equal(r["ordering"], o["ordering"])
     np.testing.assert_array_equal(r["mask"], o["mask"])
     np.testing.assert_array_equal(r["errors"], o["errors"])
