@@ -285,6 +285,8 @@ def run_ours(args, world, rank, local):
 
     sel = Selector(split.Xtrain, split.ytrain, split.Xval, split.yval, k_vals=[k], num_features=steps,
                    method="forward", device=local)
+    sel.set_pruning(args.prune)
+    sel.set_kernel(args.kernel)
     for _ in range(args.warmup):
         sel.run()
 
@@ -404,6 +406,8 @@ def main():
     ap.add_argument("--rows-scale", type=float, default=1.0,
                     help="scale n_train and n_val (small cases for profiler captures; not the bench workload)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiler captures)")
+    ap.add_argument("--prune", type=int, default=0, help="exact pruning of forward steps (library option)")
+    ap.add_argument("--kernel", type=int, default=0, help="full-scan kernel: 0 auto, 1 rows per lane, 2 row per warp")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per scoring launch, scaled to this workload (reported as roofline.traffic)")
     args = ap.parse_args()

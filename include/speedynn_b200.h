@@ -156,10 +156,10 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
                            int *commit_launches, double *total_ms, int *total_launches);
 
 /* Options:
- *   SNN_OPT_PRUNE  forward steps after the first skip training columns whose
- *                  committed distance already exceeds every candidate's bound
- *                  on its k-th neighbour distance (exact: same results);
- *                  0 forces the full scan of every column. */
+ *   SNN_OPT_PRUNE  1: forward steps after the first skip training columns
+ *                  whose committed distance already exceeds every candidate's
+ *                  bound on its k-th neighbour distance (exact: same results;
+ *                  pays off only when few columns survive).  Default 0. */
 #define SNN_OPT_PRUNE 1
 /*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic (row per warp
  *                  for k_max <= 64, else rows per lane), 1 rows per lane,

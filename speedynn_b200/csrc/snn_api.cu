@@ -74,7 +74,7 @@ struct snn_handle {
     int *seeds = nullptr;         // [n_rows][M]
     int M = 0;
     unsigned long long *survivors = nullptr;
-    bool prune = true;
+    bool prune = false;           // measured slower than the full scan on dense data; opt in
     int kernel = 0;               // scoring kernel: 0 auto, 1 rows-per-lane, 2 row-per-warp
     int max_smem = 0;
     unsigned long long scanned_pairs = 0;  // host count of (row, column) pairs the pruned path streamed

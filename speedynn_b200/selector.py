@@ -115,7 +115,7 @@ class Selector:
         return cands, idx, dist
 
     def set_pruning(self, enable):
-        """Exact pruning of forward steps after the first (on by default)."""
+        """Exact pruning of forward steps after the first (off by default)."""
         check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_PRUNE, int(bool(enable))))
 
     def set_kernel(self, which):
