@@ -7,7 +7,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libspeedynn_b200.so")
+# SNN_LIBRARY may name another build of the same library (e.g. a debug build).
+LIB_PATH = os.environ.get("SNN_LIBRARY") or os.path.join(HERE, "libspeedynn_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "speedynn_b200.h")
 
 SNN_OK = 0
