@@ -191,6 +191,9 @@ bool use_sparse(const snn_handle *h, int t, int n_cand)
            snn::sparse_smem_per_warp(n_cand, h->kmax) <= (size_t)h->max_smem;
 }
 
+// Seed columns are only needed by the pruned forward scorer.
+bool seeds_wanted(const snn_handle *h) { return h->prune && !h->desc.backward && h->M > 0; }
+
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)
 {
@@ -222,7 +225,7 @@ int issue_step(snn_handle *h, int t)
         EventPair &ce = h->commit_ev[h->n_commit];
         if (int rc = make_pair(ce)) return rc;
         SNN_CUDA(cudaEventRecord(ce.a, h->stream));
-        SNN_CUDA(snn::launch_commit_seeds(b, backward, backward ? nullptr : h->seeds, h->M, h->stream));
+        SNN_CUDA(snn::launch_commit_seeds(b, backward, seeds_wanted(h) ? h->seeds : nullptr, h->M, h->stream));
         SNN_CUDA(cudaEventRecord(ce.b, h->stream));
         h->n_commit++;
         h->n_launch += 1;
@@ -475,7 +478,7 @@ SNN_API int snn_commit_sequence(snn_handle *h, const int *seq, int n)
     for (int t = 0; t < n; ++t) {
         const int it = h->desc.backward ? h->p - 1 - t : t;
         SNN_CUDA(snn::launch_force(b, seq[t], it, t, h->total_steps, h->desc.backward, h->stream));
-        SNN_CUDA(snn::launch_commit_seeds(b, h->desc.backward, h->desc.backward ? nullptr : h->seeds, h->M, h->stream));
+        SNN_CUDA(snn::launch_commit_seeds(b, h->desc.backward, seeds_wanted(h) ? h->seeds : nullptr, h->M, h->stream));
     }
     h->host_step = n;
     SNN_CUDA(cudaStreamSynchronize(h->stream));
