@@ -45,6 +45,7 @@ extern "C" {
 #define SNN_ERR_UNSUPPORTED (-4)  /* a reference option outside this library's path */
 #define SNN_ERR_NO_WINNER (-5)    /* no candidate had an error below FLT_MAX (e.g. NaN labels) */
 #define SNN_ERR_STATE (-6)        /* call out of order (e.g. run before load) */
+#define SNN_ERR_TIMEOUT (-7)      /* a bounded wait inside a kernel gave up (pipeline stalled) */
 
 /* loss ids, speedynn/base.py:13-23 */
 #define SNN_LOSS_RMSE 0
@@ -161,10 +162,11 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
  *                  bound on its k-th neighbour distance (exact: same results;
  *                  pays off only when few columns survive).  Default 0. */
 #define SNN_OPT_PRUNE 1
-/*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic (row per warp
- *                  for k_max <= 64, else rows per lane), 1 rows per lane,
- *                  2 row per warp.  Results are identical; this exists for
- *                  cross-checks and measurement. */
+/*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic, 1 rows per
+ *                  lane (any k_max <= 256), 2 row tiles per warp (k_max <= 64),
+ *                  3 row tiles fed by a TMA/mbarrier ring (k_max <= 32).
+ *                  Results are identical; this exists for cross-checks and
+ *                  measurement. */
 #define SNN_OPT_KERNEL 2
 SNN_API int snn_set_option(snn_handle *h, int option, int value);
 

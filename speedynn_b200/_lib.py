@@ -18,6 +18,7 @@ SNN_ERR_NOMEM = -3
 SNN_ERR_UNSUPPORTED = -4
 SNN_ERR_NO_WINNER = -5
 SNN_ERR_STATE = -6
+SNN_ERR_TIMEOUT = -7
 
 SNN_OPT_PRUNE = 1
 SNN_OPT_KERNEL = 2

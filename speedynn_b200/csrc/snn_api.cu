@@ -209,6 +209,8 @@ int issue_step(snn_handle *h, int t)
         snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
         SNN_CUDA(snn::launch_score_sparse(b, sp, n_cand, h->M, h->max_smem, h->stream));
         h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
+    } else if (h->kernel == 3) {
+        SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
     } else if (h->kernel != 1 && snn::score_rw_supported(h->kmax)) {
         SNN_CUDA(snn::launch_score_rw(b, n_cand, backward, h->stream));
     } else {
@@ -434,6 +436,7 @@ SNN_API int snn_run(snn_handle *h)
     SNN_CUDA(cudaEventRecord(h->total_ev.b, h->stream));
     State s;
     if (int rc = read_state(h, &s)) return rc;
+    if (s.error == snn::kErrTimeout) return fail(SNN_ERR_TIMEOUT, "a device pipeline wait timed out at step %d", s.step);
     if (s.error) return fail(s.error, "no candidate had an error below FLT_MAX at step %d (non-finite labels?)", s.step);
     return SNN_OK;
 }
@@ -454,6 +457,7 @@ SNN_API int snn_step(snn_handle *h)
     SNN_CUDA(cudaEventRecord(h->total_ev.b, h->stream));
     h->host_step++;
     if (int rc = read_state(h, &s)) return rc;
+    if (s.error == snn::kErrTimeout) return fail(SNN_ERR_TIMEOUT, "a device pipeline wait timed out at step %d", s.step);
     if (s.error) return fail(s.error, "no candidate had an error below FLT_MAX at step %d", s.step);
     return 1;
 }
@@ -577,9 +581,11 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value)
     switch (option) {
     case SNN_OPT_PRUNE: h->prune = value != 0; return SNN_OK;
     case SNN_OPT_KERNEL:
-        if (value < 0 || value > 2) return fail(SNN_ERR_ARG, "kernel choice %d not in 0..2", value);
+        if (value < 0 || value > 3) return fail(SNN_ERR_ARG, "kernel choice %d not in 0..3", value);
         if (value == 2 && !snn::score_rw_supported(h->kmax))
-            return fail(SNN_ERR_UNSUPPORTED, "the row-per-warp kernel handles k_max <= 64");
+            return fail(SNN_ERR_UNSUPPORTED, "the row-tile kernel handles k_max <= 64");
+        if (value == 3 && !snn::score_tma_supported(h->kmax))
+            return fail(SNN_ERR_UNSUPPORTED, "the TMA-fed kernel handles k_max <= 32");
         h->kernel = value;
         return SNN_OK;
     default: return fail(SNN_ERR_ARG, "unknown option %d", option);

@@ -66,6 +66,12 @@ struct ScorePlan {
 };
 ScorePlan plan_score(int kmax, int p, int max_smem);
 
+constexpr int kErrTimeout = -7;  // SNN_ERR_TIMEOUT: a bounded device wait gave up
+
+// Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 32.
+bool score_tma_supported(int kmax);
+cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
+
 // Row-per-warp scoring (snn_score_rw.cu), k_max <= 64.
 bool score_rw_supported(int kmax);
 cudaError_t launch_score_rw(const Bufs &b, int n_cand, int backward, cudaStream_t s);

@@ -196,6 +196,49 @@ __device__ __forceinline__ float sqdiff1(float a, float b)
     return __fmul_rn(t, t);
 }
 
+// The rare path of the scoring loop, out of line so that the hot loop stays
+// small enough for the compiler to unroll and pipeline (its mere presence
+// inline cost 2.4x).  Everything it needs is in shared memory: the warp's
+// lists, thresholds and x values, and the staged D and X tiles; it recomputes
+// the passing distances with scalar .rn operations (bit-identical to the
+// packed ones) and inserts them problem by problem, lanes and columns in
+// ascending order.  `pm` is the lane's mask of problems with a passing column.
+template <int CW, bool BWD>
+__device__ __noinline__ void rare_path(unsigned pm, float *myL, int *myI, float *myT, const float *myX,
+                                       const float *D_w, const float *X_w, int q0, int colbase, int K, int KL)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned wm = __reduce_or_sync(kFull, pm);
+    while (wm) {
+        const int p = __ffs(wm) - 1;
+        wm &= wm - 1;
+        unsigned m = __ballot_sync(kFull, (pm >> p) & 1u);
+        const float *drow = D_w + (p / CW) * kStageCols + q0;
+        const float *xrow = X_w + (p % CW) * kStageCols + q0;
+        const float xv = myX[p];
+        float th = myT[p];
+        float *L = myL + p * KL;
+        int *LI = myI + p * KL;
+        while (m) {
+            const int Lh = __ffs(m) - 1;
+            m &= m - 1;
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                const int c = 2 * Lh + h;
+                const float s1 = sqdiff1(xv, xrow[c]);
+                const float d = BWD ? __fsub_rn(drow[c], s1) : __fadd_rn(drow[c], s1);
+                // inclusive threshold: T until the list is full, then just below its k-th
+                if (d <= th) {
+                    const float kth = smem_list_insert(L, LI, K, d, colbase + c, lane);
+                    if (kth < FLT_MAX) th = nextafterf(kth, -INFINITY);
+                }
+            }
+        }
+        if (lane == 0) myT[p] = th;
+        __syncwarp();
+    }
+}
+
 // Warp tile: RW scored rows x CW candidates (P = RW*CW problems, all lanes
 // walking the same columns).  Block: NRG x NCG warps = BR rows x BC
 // candidates sharing one D tile and one X tile per pipeline stage; per warp
@@ -349,6 +392,7 @@ __global__ void __launch_bounds__(NRG *NCG * 32, 1) k_score_rw(Bufs b, int n_can
             }
             continue;
         }
+#pragma unroll 2
         for (int q0 = 0; q0 < cols; q0 += kChunk) {
             float2 dp[RW], xp[CW];
 #pragma unroll
@@ -366,37 +410,7 @@ __global__ void __launch_bounds__(NRG *NCG * 32, 1) k_score_rw(Bufs b, int n_can
                     pm |= (le_mask(e.x, thr[p]) | le_mask(e.y, thr[p])) & (1u << p);
                 }
             if (__any_sync(kFull, pm != 0u)) {
-                // rare path, one compact copy: problems with a pass, lanes in order, columns in order
-                unsigned wm = __reduce_or_sync(kFull, pm);
-                const int colbase = i0 + q0;
-                while (wm) {
-                    const int p = __ffs(wm) - 1;
-                    wm &= wm - 1;
-                    unsigned m = __ballot_sync(kFull, (pm >> p) & 1u);
-                    const float *drow = D_w + (p / CW) * kStageCols + q0;
-                    const float *xrow = X_w + (p % CW) * kStageCols + q0;
-                    const float xv = myX[p];
-                    float th = myT[p];
-                    float *L = myL + p * KL;
-                    int *LI = myI + p * KL;
-                    while (m) {
-                        const int Lh = __ffs(m) - 1;
-                        m &= m - 1;
-#pragma unroll 1
-                        for (int h = 0; h < 2; ++h) {
-                            const int c = 2 * Lh + h;
-                            const float s1 = sqdiff1(xv, xrow[c]);
-                            const float d = BWD ? __fsub_rn(drow[c], s1) : __fadd_rn(drow[c], s1);
-                            // inclusive threshold: T until the list is full, then just below its k-th
-                            if (d <= th) {
-                                const float kth = smem_list_insert(L, LI, K, d, colbase + c, lane);
-                                if (kth < FLT_MAX) th = nextafterf(kth, -INFINITY);
-                            }
-                        }
-                    }
-                    if (lane == 0) myT[p] = th;
-                    __syncwarp();
-                }
+                rare_path<CW, BWD>(pm, myL, myI, myT, myX, D_w, X_w, q0, i0 + q0, K, KL);
 #pragma unroll
                 for (int p = 0; p < P; ++p) thr[p] = myT[p];
             }

@@ -108,11 +108,13 @@ def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, kernel=0, **kw):
     (700, 257, 10, 10, [64], 3, "forward"),            # k_max 64 -> 2 per thread
     (400, 130, 9, 11, [150, 2], 2, "backward"),        # k_max 150 -> 1 per thread
 ])
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_holdout_matches_oracle(args, kernel):
     n_train, n_val, p, seed, kv, nf, method = args
     if kernel == 2 and max(kv) > 64:
-        pytest.skip("the row-per-warp kernel handles k_max <= 64")
+        pytest.skip("the row-tile kernel handles k_max <= 64")
+    if kernel == 3 and max(kv) > 32:
+        pytest.skip("the TMA-fed kernel handles k_max <= 32")
     o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method, kernel=kernel)
     np.testing.assert_array_equal(r["ordering"], o["ordering"])
     np.testing.assert_array_equal(r["mask"], o["mask"])
