@@ -162,7 +162,8 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
  *                  bound on its k-th neighbour distance (exact: same results;
  *                  pays off only when few columns survive).  Default 0. */
 #define SNN_OPT_PRUNE 1
-/*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic, 1 rows per
+/*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic (3 for
+ *                  k_max <= 32, else 2 for k_max <= 64, else 1), 1 rows per
  *                  lane (any k_max <= 256), 2 row tiles per warp (k_max <= 64),
  *                  3 row tiles fed by a TMA/mbarrier ring (k_max <= 32).
  *                  Results are identical; this exists for cross-checks and

@@ -209,7 +209,7 @@ int issue_step(snn_handle *h, int t)
         snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
         SNN_CUDA(snn::launch_score_sparse(b, sp, n_cand, h->M, h->max_smem, h->stream));
         h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
-    } else if (h->kernel == 3) {
+    } else if (h->kernel == 3 || (h->kernel == 0 && snn::score_tma_supported(h->kmax))) {
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
     } else if (h->kernel != 1 && snn::score_rw_supported(h->kmax)) {
         SNN_CUDA(snn::launch_score_rw(b, n_cand, backward, h->stream));
