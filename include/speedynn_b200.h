@@ -177,6 +177,38 @@ SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, 
 
 SNN_API int snn_destroy(snn_handle *h);
 
+/* ---------------------------------------------------------------------------
+ * 3. One greedy step without device allocation
+ * ------------------------------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code running under another runtime's allocator or a fixed
+ * memory budget, hosts that forbid allocation after start-up, paths that
+ * must not let cudaMalloc/cudaFree synchronise the device -- this scores one
+ * greedy step from caller-owned DEVICE buffers and writes every candidate's
+ * RMSE for every k: errors[c * num_k_vals + m] (FP32, the reference's value)
+ * and errors64 (same residuals summed in FP64).  It never allocates: its
+ * scratch (kNN predictions, step state, copies of cands and k_vals) is a
+ * fixed 16 MB static device array, so n_cand * num_k_vals * n_rows must not
+ * exceed 4,194,304 (else SNN_ERR_ARG), num_k_vals <= 256, n_cand <= 1024.
+ *
+ * Layouts (the handle API's): D [n_rows][ld] committed distances with
+ * ld % 64 == 0, ld >= n_train and +inf in columns >= n_train (and on
+ * excluded pairs); XT [p][ld] training points feature-major; XV [p][ldr]
+ * scored points feature-major; y_train [n_train], y_val [n_rows].  cands
+ * and k_vals are HOST arrays (feature ids to score, k values).  backward=1
+ * scores removals (D - square) instead of additions.  stream: a
+ * cudaStream_t (NULL = legacy default stream); the call waits for it.
+ *
+ * The first call on each device looks up the scratch's device address
+ * (with that device current); make that first call before any stream
+ * capture.  All calls share the scratch and it keeps the last call's
+ * contents: calls whose GPU work overlaps race on it. */
+SNN_API int snn_score_step_noalloc(const float *D, int ld, const float *XT, const float *XV, int ldr,
+                                   const float *y_train, const float *y_val, int n_rows, int n_train, int p,
+                                   const int *cands, int n_cand, const int *k_vals, int num_k_vals, int backward,
+                                   float *errors, double *errors64, void *stream);
+
 /* Message of the last failure on the calling thread ("" if none). */
 SNN_API const char *snn_last_error(void);
 

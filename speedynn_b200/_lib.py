@@ -82,6 +82,9 @@ def lib():
             "train_backward_selection": (ctypes.c_int, [_f32p, ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int, _i32p,
                                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int,
                                                         ctypes.c_int, ctypes.c_int]),
+            "snn_score_step_noalloc": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int,
+                                                      ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, _i32p,
+                                                      ctypes.c_int, ctypes.c_int, vp, vp, vp]),
             "get_selected_dimensions": (None, [_i32p, ctypes.c_int]),
             "get_selected_ordering": (None, [_i32p, ctypes.c_int]),
             "get_selected_errors": (None, [_f32p, ctypes.c_int]),

@@ -54,6 +54,16 @@ struct EventPair {
 
 }  // namespace
 
+namespace snn {
+// Record a failure for snn_last_error() from another translation unit.
+int record_error(int code, const char *msg)
+{
+    g_err = msg;
+    return code;
+}
+void clear_error() { g_err.clear(); }
+}  // namespace snn
+
 struct snn_handle {
     snn_desc desc{};
     std::vector<int> kvals;

@@ -68,6 +68,10 @@ ScorePlan plan_score(int kmax, int p, int max_smem);
 
 constexpr int kErrTimeout = -7;  // SNN_ERR_TIMEOUT: a bounded device wait gave up
 
+// snn_last_error() plumbing shared by the C-ABI translation units.
+int record_error(int code, const char *msg);
+void clear_error();
+
 // Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 32.
 bool score_tma_supported(int kmax);
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
