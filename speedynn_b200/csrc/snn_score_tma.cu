@@ -19,9 +19,13 @@
 // of the columns gives an inclusive bound T (k-th smallest of per-lane
 // minima = the distance of k distinct columns), the full pass inserts d <= T
 // until the list is full and then d < k-th, columns in ascending order.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <float.h>
 #include <math.h>
 #include <stdint.h>
+
+#include <mutex>
 
 #include "snn_internal.h"
 
@@ -63,6 +67,38 @@ __device__ __forceinline__ float2 sq2(float2 t)
     asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(d) : "l"(as_u64(t)), "l"(z));
     return as_f2(d);
 }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)), "l"(as_u64(c)));
+    return as_f2(d);
+}
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ unsigned f2u(float v) { return __float_as_uint(v); }
+
+// Inclusive bound on the exact forward distance from a first-pass value
+// a = fl(t*t + D), D >= 0: d = fl(D + fl(t*t)) <= a (1 + 3.01 * 2^-24) + 2^-147,
+// and fma(a, 1 + 2^-20, 2^-140) exceeds that after its own rounding.  Capped
+// at the largest float below FLT_MAX (items at FLT_MAX never enter a list).
+__device__ __forceinline__ float fwd_bound(float a)
+{
+    return fminf(fmaf(a, 1.0f + 0x1p-20f, 0x1p-140f), 0x1.fffffcp+127f);
+}
+
+// Filter bound H for an inclusive threshold T (forward, D >= 0).  If
+// d = fl(D + fl(t*t)) <= T then the exact value t*t + fl(D - H) is negative:
+// D + t*t <= T+ (1 + 2^-23) + 2^-149 with T+ = max(T, 0), fl(D - H) is off by
+// at most H * 2^-24 + 2^-150 because 0 <= D <= H, and H >= T+ (1 + 2^-19) +
+// 2^-126 after rounding.  A negative exact value keeps its sign bit through
+// the FMA's rounding (an underflow gives -0), so testing the sign bit of
+// u = fma(t, t, fl(D - H)) never misses a passing column.
+__device__ __forceinline__ float filter_bound(float T) { return fmaf(fmaxf(T, 0.0f), 1.0f + 0x1p-18f, 0x1p-125f); }
+
 __device__ __forceinline__ unsigned le_mask(float a, float b)
 {
     unsigned r;
@@ -118,12 +154,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
     }
     return false;
 }
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+// One 2-D tile (box of the tensor map) into shared memory, completing on bar.
+__device__ __forceinline__ void tma_tile_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
 {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+// Four rows y0..y3 of a 2-D tensor (box one row high), columns x.., stacked in
+// shared memory in that order, completing on bar.
+__device__ __forceinline__ void tma_gather4(void *dst, const CUtensorMap *map, int x, int y0, int y1, int y2, int y3,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cta.global.tile::gather4.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+        "%6}], [%7];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3), "r"(smem_addr(bar))
+        : "memory");
 }
 
 // Insert (v, col) into the sorted list Ld/Li[0..K) with all 32 lanes; the
@@ -241,7 +290,8 @@ __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL)
 }
 
 template <bool BWD>
-__global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg)
+__global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg, const __grid_constant__ CUtensorMap tmD,
+                                                                   const __grid_constant__ CUtensorMap tmX)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int K = b.kmax;
@@ -272,38 +322,37 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     const int nvirt = nA + nstages;
 
     if (w == kConsumers) {
-        // ---------------- producer warp ----------------
-        const int rlast = b.n_rows - 1;
-        int issued = 0;
-        bool ok = true;
-        for (int v = 0; v < nvirt; ++v) {
-            const int s = v % kRing;
-            if (!mbar_wait(S.empty + s, ((v / kRing) & 1) ^ 1)) {
-                ok = false;
-                break;
+        // ---------------- producer warp (one lane) ----------------
+        // Per stage: the D tile (kRowsB rows x kSC columns, rows past n_rows
+        // read as 0 and belong to padded problems) and the block's kCandB
+        // candidate rows of X, gathered four at a time.  Columns past ldc in the
+        // last stage also read as 0; consumers never look past ldc.
+        if (lane == 0) {
+            constexpr unsigned kStageBytes = sizeof(float) * kSC * (kRowsB + kCandB);
+            int issued = 0;
+            bool ok = true;
+            for (int v = 0; v < nvirt; ++v) {
+                const int s = v % kRing;
+                if (!mbar_wait(S.empty + s, ((v / kRing) & 1) ^ 1)) {
+                    ok = false;
+                    break;
+                }
+                const int i0 = (v < nA ? v : v - nA) * kSC;
+                mbar_arrive_expect_tx(S.full + s, kStageBytes);
+                tma_tile_2d(S.Ds + s * kRowsB * kSC, &tmD, i0, r0, S.full + s);
+#pragma unroll
+                for (int g = 0; g < kCandB / 4; ++g)
+                    tma_gather4(S.Xs + (s * kCandB + 4 * g) * kSC, &tmX, i0, S.srcand[4 * g], S.srcand[4 * g + 1],
+                                S.srcand[4 * g + 2], S.srcand[4 * g + 3], S.full + s);
+                issued = v + 1;
             }
-            const int st = v < nA ? v : v - nA;
-            const int i0 = st * kSC;
-            const int ncols = min(kSC, b.ldc - i0);
-            const unsigned bytes = (unsigned)ncols * 4u;
-            if (lane == 0) mbar_arrive_expect_tx(S.full + s, bytes * (kRowsB + kCandB));
-            __syncwarp();
-            if (lane < kRowsB) {
-                const int rr = min(r0 + lane, rlast);
-                bulk_g2s(S.Ds + (s * kRowsB + lane) * kSC, b.D + (size_t)rr * b.ldc + i0, bytes, S.full + s);
-            } else {
-                const int c = lane - kRowsB;
-                bulk_g2s(S.Xs + (s * kCandB + c) * kSC, b.XT + (size_t)S.srcand[c] * b.ldc + i0, bytes, S.full + s);
-            }
-            issued = v + 1;
-        }
-        if (!ok) {
-            if (lane == 0) {
+            if (!ok) {
                 atomicExch(&b.st->error, kErrTimeout);
                 atomicExch(&b.st->done, 1);
+                // drain: wait (bounded) for the copies of the stages still in flight
+                for (int v = issued > kRing ? issued - kRing : 0; v < issued; ++v)
+                    mbar_wait(S.full + v % kRing, (v / kRing) & 1);
             }
-            // drain: wait (bounded) for the copies of the stages still in flight
-            for (int v = issued > kRing ? issued - kRing : 0; v < issued; ++v) mbar_wait(S.full + v % kRing, (v / kRing) & 1);
         }
         return;
     }
@@ -321,8 +370,11 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
         myL[e] = (e % KL) < K ? FLT_MAX : INFINITY;
         myI[e] = 0;
     }
+    // A padded problem (row past n_rows or candidate slot past n_cand) gets a
+    // scored value that can never pass: NaN for backward (d = NaN), +inf for
+    // forward (d = D + inf = inf, and the forward filter value stays >= 0).
     float2 xv2[kP];
-    float thr[kP];
+    unsigned okmask = 0u;
 #pragma unroll
     for (int ri = 0; ri < kRW; ++ri)
 #pragma unroll
@@ -330,14 +382,18 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
             const int p = ri * kCW + ci;
             const int r = wr0 + ri;
             const bool okp = r < b.n_rows && c0 + wc + ci < n_cand;
-            const float x = okp ? __ldg(b.XV + (size_t)S.srcand[wc + ci] * b.ldr + r) : NAN;  // NaN never passes
+            const float x = okp ? __ldg(b.XV + (size_t)S.srcand[wc + ci] * b.ldr + r) : (BWD ? NAN : INFINITY);
             xv2[p] = make_float2(x, x);
+            okmask |= okp ? (1u << p) : 0u;
             if (lane == 0) myX[p] = x;
         }
     __syncwarp();
 
     bool alive = true;
-    // first pass: per-lane minimum per problem over nA stages
+    // First pass over nA stages: per-lane minimum per problem.  Backward takes
+    // the exact distance; forward takes a = fl(t*t + D) (one FMA), which is at
+    // most 3 ulp below the exact d = fl(D + fl(t*t)) for D >= 0, so the bound
+    // derived from it is widened by 2^-20 relative (see fwd_bound).
     {
         float mn[kP];
 #pragma unroll
@@ -365,64 +421,146 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
 #pragma unroll
                         for (int ci = 0; ci < kCW; ++ci) {
                             const int p = ri * kCW + ci;
-                            const float2 s2 = sq2(sub2(xv2[p], xp[ci]));
-                            const float2 e = BWD ? sub2(dp[ri], s2) : add2(dp[ri], s2);
-                            mn[p] = fminf(mn[p], fminf(e.x, e.y));
+                            const float2 t = sub2(xv2[p], xp[ci]);
+                            float2 e;
+                            if constexpr (BWD) e = sub2(dp[ri], sq2(t));
+                            else e = fma2(t, t, dp[ri]);
+                            mn[p] = min3f(mn[p], e.x, e.y);
                         }
                 }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(S.empty + s);
         }
-        // T = k-th smallest of the 32 lane minima (k <= 32): the distance of k distinct columns
+        // T = k-th smallest of the 32 lane minima (k <= 32): k distinct columns lie at or below it
 #pragma unroll
         for (int p = 0; p < kP; ++p) {
             const float srt = warp_sort32(mn[p], lane);
             const float T = __shfl_sync(kFull, srt, (K - 1) & 31);
-            thr[p] = T < FLT_MAX ? T : nextafterf(FLT_MAX, 0.0f);  // inclusive bound
-            if (lane == 0) myT[p] = thr[p];
+            float th;
+            if constexpr (BWD) th = T < FLT_MAX ? T : nextafterf(FLT_MAX, 0.0f);  // inclusive bound
+            else th = (okmask >> p) & 1u ? fwd_bound(T) : -1.0f;                // padded: never passes
+            if (lane == 0) myT[p] = th;
         }
         __syncwarp();
     }
 
-    // full pass
-    for (int v = nA; v < nvirt && alive; ++v) {
-        const int s = v % kRing;
-        if (!mbar_wait(S.full + s, (v / kRing) & 1)) {
-            alive = false;
-            break;
-        }
-        const int i0 = (v - nA) * kSC;
-        const int cols = min(kSC, b.ldc - i0);
-        const float *D_w = S.Ds + (s * kRowsB + rg * kRW) * kSC;
-        const float *X_w = S.Xs + (s * kCandB + wc) * kSC;
-        if (wvalid) {
+    if constexpr (!BWD) {
+        // Forward full pass through a conservative filter.  Per scored row the
+        // warp keeps H = the largest filter_bound() of its four problems; a
+        // column can pass (d <= threshold) only if u = fl(t*t + fl(D - H)) < 0,
+        // so the hot loop costs one sub and one FMA per evaluation plus an OR
+        // of sign bits.  A chunk with a set sign bit is re-scored exactly.
+        float2 H2[kRW];
+        auto load_H = [&]() {
+#pragma unroll
+            for (int ri = 0; ri < kRW; ++ri) {
+                const float h = fmaxf(fmaxf(filter_bound(myT[ri * kCW + 0]), filter_bound(myT[ri * kCW + 1])),
+                                      fmaxf(filter_bound(myT[ri * kCW + 2]), filter_bound(myT[ri * kCW + 3])));
+                H2[ri] = make_float2(h, h);
+            }
+        };
+        load_H();
+        for (int v = nA; v < nvirt && alive; ++v) {
+            const int s = v % kRing;
+            if (!mbar_wait(S.full + s, (v / kRing) & 1)) {
+                alive = false;
+                break;
+            }
+            const int i0 = (v - nA) * kSC;
+            const int cols = min(kSC, b.ldc - i0);
+            const float *D_w = S.Ds + (s * kRowsB + rg * kRW) * kSC;
+            const float *X_w = S.Xs + (s * kCandB + wc) * kSC;
+            if (wvalid) {
 #pragma unroll 2
-            for (int q0 = 0; q0 < cols; q0 += kChunk) {
-                float2 dp[kRW], xp[kCW];
+                for (int q0 = 0; q0 < cols; q0 += kChunk) {
+                    float2 dp[kRW], xp[kCW];
 #pragma unroll
-                for (int ri = 0; ri < kRW; ++ri) dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0 + 2 * lane);
+                    for (int ri = 0; ri < kRW; ++ri)
+                        dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0 + 2 * lane);
 #pragma unroll
-                for (int ci = 0; ci < kCW; ++ci) xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0 + 2 * lane);
-                unsigned pm = 0u;
+                    for (int ci = 0; ci < kCW; ++ci)
+                        xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0 + 2 * lane);
+                    unsigned acc[kRW];
 #pragma unroll
-                for (int ri = 0; ri < kRW; ++ri)
+                    for (int ri = 0; ri < kRW; ++ri) {
+                        const float2 E = sub2(dp[ri], H2[ri]);
+                        float2 u[kCW];
 #pragma unroll
-                    for (int ci = 0; ci < kCW; ++ci) {
-                        const int p = ri * kCW + ci;
-                        const float2 s2 = sq2(sub2(xv2[p], xp[ci]));
-                        const float2 e = BWD ? sub2(dp[ri], s2) : add2(dp[ri], s2);
-                        pm |= (le_mask(e.x, thr[p]) | le_mask(e.y, thr[p])) & (1u << p);
+                        for (int ci = 0; ci < kCW; ++ci) {
+                            const float2 t = sub2(xv2[ri * kCW + ci], xp[ci]);
+                            u[ci] = fma2(t, t, E);
+                        }
+                        acc[ri] = (f2u(u[0].x) | f2u(u[0].y) | f2u(u[1].x)) | (f2u(u[1].y) | f2u(u[2].x) | f2u(u[2].y)) |
+                                  (f2u(u[3].x) | f2u(u[3].y));
                     }
-                if (__any_sync(kFull, pm != 0u)) {
-                    rare_path<BWD>(pm, myL, myI, myT, myX, D_w, X_w, q0, i0 + q0, K, KL);
+                    const unsigned any_sign = (acc[0] | acc[1]) | (acc[2] | acc[3]);
+                    if (__any_sync(kFull, (int)any_sign < 0)) {
+                        // exact pass mask for this chunk (reference rounding), then insert
+                        unsigned pm = 0u;
 #pragma unroll
-                    for (int p = 0; p < kP; ++p) thr[p] = myT[p];
+                        for (int ri = 0; ri < kRW; ++ri)
+#pragma unroll
+                            for (int ci = 0; ci < kCW; ++ci) {
+                                const int p = ri * kCW + ci;
+                                const float th = myT[p];
+                                const float2 e = add2(dp[ri], sq2(sub2(xv2[p], xp[ci])));
+                                pm |= (le_mask(e.x, th) | le_mask(e.y, th)) & (1u << p);
+                            }
+                        if (__any_sync(kFull, pm != 0u)) {
+                            rare_path<false>(pm, myL, myI, myT, myX, D_w, X_w, q0, i0 + q0, K, KL);
+                            load_H();
+                        }
+                    }
                 }
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(S.empty + s);
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(S.empty + s);
+    } else {
+        // Backward full pass: exact distances, threshold compare per element.
+        float thr[kP];
+#pragma unroll
+        for (int p = 0; p < kP; ++p) thr[p] = myT[p];
+        for (int v = nA; v < nvirt && alive; ++v) {
+            const int s = v % kRing;
+            if (!mbar_wait(S.full + s, (v / kRing) & 1)) {
+                alive = false;
+                break;
+            }
+            const int i0 = (v - nA) * kSC;
+            const int cols = min(kSC, b.ldc - i0);
+            const float *D_w = S.Ds + (s * kRowsB + rg * kRW) * kSC;
+            const float *X_w = S.Xs + (s * kCandB + wc) * kSC;
+            if (wvalid) {
+#pragma unroll 2
+                for (int q0 = 0; q0 < cols; q0 += kChunk) {
+                    float2 dp[kRW], xp[kCW];
+#pragma unroll
+                    for (int ri = 0; ri < kRW; ++ri)
+                        dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0 + 2 * lane);
+#pragma unroll
+                    for (int ci = 0; ci < kCW; ++ci)
+                        xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0 + 2 * lane);
+                    unsigned pm = 0u;
+#pragma unroll
+                    for (int ri = 0; ri < kRW; ++ri)
+#pragma unroll
+                        for (int ci = 0; ci < kCW; ++ci) {
+                            const int p = ri * kCW + ci;
+                            const float2 e = sub2(dp[ri], sq2(sub2(xv2[p], xp[ci])));
+                            pm |= (le_mask(e.x, thr[p]) | le_mask(e.y, thr[p])) & (1u << p);
+                        }
+                    if (__any_sync(kFull, pm != 0u)) {
+                        rare_path<true>(pm, myL, myI, myT, myX, D_w, X_w, q0, i0 + q0, K, KL);
+#pragma unroll
+                        for (int p = 0; p < kP; ++p) thr[p] = myT[p];
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(S.empty + s);
+        }
     }
     if (!alive) {
         if (lane == 0) {
@@ -433,29 +571,37 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     }
     if (!wvalid) return;
 
-    const int nk = b.nk;
-    for (int p = 0; p < kP; ++p) {
-        const int r = wr0 + p / kCW;
-        const int slot = c0 + wc + p % kCW;
-        if (r >= b.n_rows || slot >= n_cand) continue;
-        const float *L = myL + p * KL;
-        const int *LI = myI + p * KL;
-        if (b.nn_idx) {
+    // Epilogue: optional neighbour dump, then labels gathered by all lanes and
+    // summed in rank order (sequential FP32, as the reference) by lane p.
+    if (b.nn_idx) {
+        for (int p = 0; p < kP; ++p) {
+            const int r = wr0 + p / kCW;
+            const int slot = c0 + wc + p % kCW;
+            if (!((okmask >> p) & 1u)) continue;
             const size_t o = ((size_t)slot * b.n_rows + r) * K;
             for (int x = lane; x < K; x += 32) {
-                b.nn_idx[o + x] = LI[x];
-                b.nn_dist[o + x] = L[x];
+                b.nn_idx[o + x] = myI[p * KL + x];
+                b.nn_dist[o + x] = myL[p * KL + x];
             }
         }
-        // label sum in rank order (sequential FP32, as the reference), lane 0
-        if (lane == 0) {
-            float acc = 0.0f;
-            for (int j = 0; j < K; ++j) {
-                acc = __fadd_rn(acc, __ldg(b.yc + LI[j]));
-                for (int m = 0; m < nk; ++m) {
-                    const int k = __ldg(b.kvals + m);
-                    if (k == j + 1) b.pred[((size_t)slot * nk + m) * b.n_rows + r] = __fdiv_rn(acc, (float)k);
-                }
+        __syncwarp();
+    }
+    for (int e = lane; e < kP * K; e += 32) {
+        const int p = e / K, j = e - p * K;
+        if ((okmask >> p) & 1u) myL[p * KL + j] = __ldg(b.yc + myI[p * KL + j]);
+    }
+    __syncwarp();
+    if (lane < kP && ((okmask >> lane) & 1u)) {
+        const int p = lane;
+        const int r = wr0 + p / kCW;
+        const int slot = c0 + wc + p % kCW;
+        const int nk = b.nk;
+        float acc = 0.0f;
+        for (int j = 0; j < K; ++j) {
+            acc = __fadd_rn(acc, myL[p * KL + j]);
+            for (int m = 0; m < nk; ++m) {
+                const int k = __ldg(b.kvals + m);
+                if (k == j + 1) b.pred[((size_t)slot * nk + m) * b.n_rows + r] = __fdiv_rn(acc, (float)k);
             }
         }
     }
@@ -473,16 +619,53 @@ size_t tma_smem_bytes(int K)
 
 bool score_tma_supported(int kmax) { return kmax >= 1 && kmax <= 32; }
 
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// Row-major FP32 matrix [rows][ld] (ld a multiple of 4, base 16-byte aligned)
+// as a 2-D tensor map with a box of box_rows x kSC; out-of-range reads give 0.
+bool encode_rows(CUtensorMap *m, const float *base, int ld, long long rows, int box_rows)
+{
+    const PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn || (reinterpret_cast<uintptr_t>(base) & 15u) || ld % 4) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kSC, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s)
 {
     const int n_cg = (n_cand + kCandB - 1) / kCandB;
     const long long blocks = (long long)((b.n_rows + kRowsB - 1) / kRowsB) * n_cg;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    CUtensorMap tmD, tmX;
+    if (!encode_rows(&tmD, b.D, b.ldc, b.n_rows, kRowsB) || !encode_rows(&tmX, b.XT, b.ldc, b.p, 1))
+        return cudaErrorInvalidValue;
     const size_t smem = tma_smem_bytes(b.kmax);
     auto kern = backward ? k_score_tma<true> : k_score_tma<false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(unsigned)blocks, (kConsumers + 1) * 32, smem, s>>>(b, n_cand, n_cg);
+    kern<<<(unsigned)blocks, (kConsumers + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);
     return cudaGetLastError();
 }
 
