@@ -247,6 +247,66 @@ __device__ __noinline__ void rare_path(unsigned pm, float *myL, int *myI, float 
     }
 }
 
+// Insert a chunk's passing distances into the warp's lists (forward,
+// K <= 32).  pm holds this lane's passes, bit 2*p + h for problem p and chunk
+// column 2*lane + h; D_s / X_s are the warp's D rows and candidate X rows of
+// the stage (kSC columns each).  Items go in column order with the reference
+// rule (after every element <= d, entry below the k-th once the list is
+// full); every lane recomputes each item's exact distance from shared
+// memory, and the list being filled sits in registers, lane j holding entry j.
+__device__ __noinline__ void insert_chunk(unsigned pm, const float *D_s, const float *X_s, const float *myX, float *myL,
+                                          int *myI, float *myT, int q0, int colbase, int K, int KL)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned any = __reduce_or_sync(kFull, pm);
+    while (any) {
+        const int p = (__ffs(any) - 1) >> 1;
+        any &= ~(3u << (2 * p));
+        float *L = myL + p * KL;
+        int *LI = myI + p * KL;
+        float Lj = lane < K ? L[lane] : INFINITY;
+        int Ij = lane < K ? LI[lane] : 0;
+        float th = myT[p];
+        const float xv = myX[p];
+        const float *xrow = X_s + (p % kCW) * kSC + q0;
+        const float *dr = D_s + (p / kCW) * kSC + q0;
+        const unsigned mine = (pm >> (2 * p)) & 3u;
+        unsigned m = __ballot_sync(kFull, mine != 0u);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const unsigned hb = __shfl_sync(kFull, mine, l);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!((hb >> h) & 1u)) continue;
+                const int c = 2 * l + h;
+                const float d = __fadd_rn(dr[c], sqdiff1(xv, xrow[c]));
+                if (d <= th) {
+                    // d < FLT_MAX and, for a full list, d < k-th: the slot is < K
+                    const int pos = __popc(__ballot_sync(kFull, lane < K && Lj <= d));
+                    const float upL = __shfl_up_sync(kFull, Lj, 1);
+                    const int upI = __shfl_up_sync(kFull, Ij, 1);
+                    if (lane == pos) {
+                        Lj = d;
+                        Ij = colbase + c;
+                    } else if (lane > pos) {
+                        Lj = upL;
+                        Ij = upI;
+                    }
+                    const float kth = __shfl_sync(kFull, Lj, K - 1);
+                    if (kth < FLT_MAX) th = nextafterf(kth, -INFINITY);
+                }
+            }
+        }
+        if (lane < K) {
+            L[lane] = Lj;
+            LI[lane] = Ij;
+        }
+        if (lane == 0) myT[p] = th;
+    }
+    __syncwarp();
+}
+
 // Ascending bitonic sort of 32 values over the warp.
 __device__ __forceinline__ float warp_sort32(float v, int lane)
 {
@@ -450,7 +510,7 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
         // warp keeps H = the largest filter_bound() of its four problems; a
         // column can pass (d <= threshold) only if u = fl(t*t + fl(D - H)) < 0,
         // so the hot loop costs one sub and one FMA per evaluation plus an OR
-        // of sign bits.  A chunk with a set sign bit is re-scored exactly.
+        // of sign bits.  A row with a set sign bit is re-scored exactly.
         float2 H2[kRW];
         auto load_H = [&]() {
 #pragma unroll
@@ -468,19 +528,21 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                 break;
             }
             const int i0 = (v - nA) * kSC;
-            const int cols = min(kSC, b.ldc - i0);
-            const float *D_w = S.Ds + (s * kRowsB + rg * kRW) * kSC;
-            const float *X_w = S.Xs + (s * kCandB + wc) * kSC;
+            const float *D_s = S.Ds + (s * kRowsB + rg * kRW) * kSC;
+            const float *X_s = S.Xs + (s * kCandB + wc) * kSC;
+            const float *D_w = D_s + 2 * lane;
+            const float *X_w = X_s + 2 * lane;
             if (wvalid) {
-#pragma unroll 2
-                for (int q0 = 0; q0 < cols; q0 += kChunk) {
+                const int nch = b.ldc - i0 >= kSC ? kSC / kChunk : 1;  // ldc is a multiple of kChunk
+#pragma unroll 1
+                for (int q = 0; q < kSC / kChunk; ++q) {
+                    if (q >= nch) break;
+                    const int q0 = q * kChunk;
                     float2 dp[kRW], xp[kCW];
 #pragma unroll
-                    for (int ri = 0; ri < kRW; ++ri)
-                        dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0 + 2 * lane);
+                    for (int ri = 0; ri < kRW; ++ri) dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0);
 #pragma unroll
-                    for (int ci = 0; ci < kCW; ++ci)
-                        xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0 + 2 * lane);
+                    for (int ci = 0; ci < kCW; ++ci) xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0);
                     unsigned acc[kRW];
 #pragma unroll
                     for (int ri = 0; ri < kRW; ++ri) {
@@ -494,21 +556,22 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                         acc[ri] = (f2u(u[0].x) | f2u(u[0].y) | f2u(u[1].x)) | (f2u(u[1].y) | f2u(u[2].x) | f2u(u[2].y)) |
                                   (f2u(u[3].x) | f2u(u[3].y));
                     }
-                    const unsigned any_sign = (acc[0] | acc[1]) | (acc[2] | acc[3]);
-                    if (__any_sync(kFull, (int)any_sign < 0)) {
-                        // exact pass mask for this chunk (reference rounding), then insert
-                        unsigned pm = 0u;
+                    if (__any_sync(kFull, (int)((acc[0] | acc[1]) | (acc[2] | acc[3])) < 0)) {
+                        unsigned pm = 0u;  // bit 2p+h: column 2*lane+h passes problem p exactly
 #pragma unroll
-                        for (int ri = 0; ri < kRW; ++ri)
+                        for (int ri = 0; ri < kRW; ++ri) {
+                            if (__any_sync(kFull, (int)acc[ri] < 0)) {
 #pragma unroll
-                            for (int ci = 0; ci < kCW; ++ci) {
-                                const int p = ri * kCW + ci;
-                                const float th = myT[p];
-                                const float2 e = add2(dp[ri], sq2(sub2(xv2[p], xp[ci])));
-                                pm |= (le_mask(e.x, th) | le_mask(e.y, th)) & (1u << p);
+                                for (int ci = 0; ci < kCW; ++ci) {
+                                    const int p = ri * kCW + ci;
+                                    const float th = myT[p];
+                                    const float2 e = add2(dp[ri], sq2(sub2(xv2[p], xp[ci])));
+                                    pm |= (le_mask(e.x, th) & (1u << (2 * p))) | (le_mask(e.y, th) & (2u << (2 * p)));
+                                }
                             }
+                        }
                         if (__any_sync(kFull, pm != 0u)) {
-                            rare_path<false>(pm, myL, myI, myT, myX, D_w, X_w, q0, i0 + q0, K, KL);
+                            insert_chunk(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K, KL);
                             load_H();
                         }
                     }
