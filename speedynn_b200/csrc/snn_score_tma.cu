@@ -1,24 +1,27 @@
 // snn_score_tma.cu -- candidate scoring, warp-specialised TMA pipeline.
 //
-// Same contract and warp tiling as snn_score_rw.cu (exact top-k_max lists in
-// the reference's stable (distance, index) order, kNN-mean predictions; a
-// consumer warp owns 4 scored rows x 4 candidates and walks the columns two
-// per lane with packed f32x2), different feeding:
+// Contract as snn_score_rw.cu: exact top-k_max lists (k <= 32) in the
+// reference's stable (distance, index) order and kNN-mean predictions.  A
+// block scores 16 rows x 16 candidates; each of its 16 consumer warps owns 4
+// rows x 4 candidates and walks the columns two per lane with packed f32x2.
 //
-//   * one producer warp streams each 128-column stage with bulk TMA copies
-//     (cp.async.bulk ... mbarrier::complete_tx): 16 rows of D and the 16
-//     candidates' slices of X, 512 bytes each, into an 8-stage ring;
-//   * each stage has a "full" mbarrier (producer arrive + expected bytes) and
-//     an "empty" mbarrier (one arrive per consumer warp); consumers never meet
-//     at a block barrier, so a warp busy inserting falls behind by up to eight
-//     stages without stalling the other fifteen;
-//   * every wait is bounded: on timeout the warp records SNN_ERR_TIMEOUT in
+//   * Feed: one producer lane streams 256-column stages into a ring of
+//     shared-memory slots (as deep as fits beside the lists, at most 8): a
+//     2-D tensor-map TMA copy of the 16 D rows and four tile::gather4 copies
+//     of the 16 candidate rows of X, all completing on the stage's "full"
+//     mbarrier; consumers release a slot through its "empty" mbarrier, so a
+//     warp busy inserting falls behind by up to a ring of stages without
+//     stalling the others.
+//   * First pass over a quarter of the columns: per-lane minima; their k-th
+//     smallest bounds the final k-th distance (k distinct columns lie at or
+//     below it).
+//   * Full pass, forward: a conservative sign-bit filter (one sub and one FMA
+//     per evaluation, see filter_bound) flags rows that may hold a passing
+//     column; flagged rows are re-scored with the reference's rounding and
+//     passes are inserted in column order (d <= T until the list is full,
+//     then d < k-th).  Backward: exact distances and a compare per element.
+//   * Every wait is bounded: on timeout the warp records SNN_ERR_TIMEOUT in
 //     the device state and leaves (the producer first drains its copies).
-//
-// Exactness notes are those of snn_score_rw.cu: the first pass over a quarter
-// of the columns gives an inclusive bound T (k-th smallest of per-lane
-// minima = the distance of k distinct columns), the full pass inserts d <= T
-// until the list is full and then d < k-th, columns in ascending order.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <float.h>
@@ -35,14 +38,19 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kChunk = 64;        // columns per warp step (2 per lane)
-constexpr int kSC = 128;          // columns per stage
-constexpr int kRing = 8;          // stages in the ring
+constexpr int kSC = 256;          // columns per stage
+constexpr int kMaxRing = 8;       // most stages in the ring (the depth is a template argument)
+constexpr int kBarBytes = 128;    // full + empty mbarriers, padded so the tiles stay 128-byte aligned
+static_assert(2 * kMaxRing * sizeof(uint64_t) <= kBarBytes, "mbarriers must fit their area");
 constexpr int kRowsB = 16;        // scored rows per block
 constexpr int kCandB = 16;        // candidates per block
 constexpr int kConsumers = 16;    // consumer warps (4 row groups x 4 candidate groups)
 constexpr int kRW = 4, kCW = 4, kP = kRW * kCW;
 constexpr long long kSpinLimit = 1ll << 22;  // try_wait polls before giving up
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one second
+
+// Shared-memory slots per neighbour list (k <= 32).
+__host__ __device__ constexpr int list_slots(int K) { return K <= 16 ? 16 : 32; }
 
 __device__ __forceinline__ unsigned long long as_u64(float2 v) { return *reinterpret_cast<unsigned long long *>(&v); }
 __device__ __forceinline__ float2 as_f2(unsigned long long v) { return *reinterpret_cast<float2 *>(&v); }
@@ -247,6 +255,10 @@ __device__ __noinline__ void rare_path(unsigned pm, float *myL, int *myI, float 
     }
 }
 
+// Largest float below x for 0 <= x < FLT_MAX (forward distances): turns the
+// strict test d < kth into the inclusive d <= below(kth).
+__device__ __forceinline__ float below(float x) { return x > 0.0f ? __int_as_float(__float_as_int(x) - 1) : -0x1p-149f; }
+
 // Insert a chunk's passing distances into the warp's lists (forward,
 // K <= 32).  pm holds this lane's passes, bit 2*p + h for problem p and chunk
 // column 2*lane + h; D_s / X_s are the warp's D rows and candidate X rows of
@@ -254,10 +266,13 @@ __device__ __noinline__ void rare_path(unsigned pm, float *myL, int *myI, float 
 // rule (after every element <= d, entry below the k-th once the list is
 // full); every lane recomputes each item's exact distance from shared
 // memory, and the list being filled sits in registers, lane j holding entry j.
-__device__ __noinline__ void insert_chunk(unsigned pm, const float *D_s, const float *X_s, const float *myX, float *myL,
+// Returns a mask of the warp's rows (bit p / kCW) whose thresholds may have
+// changed.
+__device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, const float *X_s, const float *myX, float *myL,
                                           int *myI, float *myT, int q0, int colbase, int K, int KL)
 {
     const int lane = threadIdx.x & 31;
+    unsigned rows = 0u;
     unsigned any = __reduce_or_sync(kFull, pm);
     while (any) {
         const int p = (__ffs(any) - 1) >> 1;
@@ -294,7 +309,7 @@ __device__ __noinline__ void insert_chunk(unsigned pm, const float *D_s, const f
                         Ij = upI;
                     }
                     const float kth = __shfl_sync(kFull, Lj, K - 1);
-                    if (kth < FLT_MAX) th = nextafterf(kth, -INFINITY);
+                    if (kth < FLT_MAX) th = below(kth);
                 }
             }
         }
@@ -303,8 +318,10 @@ __device__ __noinline__ void insert_chunk(unsigned pm, const float *D_s, const f
             LI[lane] = Ij;
         }
         if (lane == 0) myT[p] = th;
+        rows |= 1u << (p / kCW);
     }
     __syncwarp();
+    return rows;
 }
 
 // Ascending bitonic sort of 32 values over the warp.
@@ -331,16 +348,16 @@ struct TmaSmem {
     int *flag;
 };
 
-__device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL)
+__device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL, int ring)
 {
     TmaSmem S;
     uint64_t *bars = reinterpret_cast<uint64_t *>(base);
     S.full = bars;
-    S.empty = bars + kRing;
-    float *f = reinterpret_cast<float *>(bars + 2 * kRing);
-    S.Ds = f;                                        // [kRing][kRowsB][kSC]
-    S.Xs = S.Ds + kRing * kRowsB * kSC;               // [kRing][kCandB][kSC]
-    S.Lds = S.Xs + kRing * kCandB * kSC;              // [kConsumers][kP][KL]
+    S.empty = bars + ring;
+    float *f = reinterpret_cast<float *>(base + kBarBytes);  // tiles start 128-byte aligned
+    S.Ds = f;                                        // [ring][kRowsB][kSC]
+    S.Xs = S.Ds + ring * kRowsB * kSC;                // [ring][kCandB][kSC]
+    S.Lds = S.Xs + ring * kCandB * kSC;               // [kConsumers][kP][KL]
     S.Lis = reinterpret_cast<int *>(S.Lds + kConsumers * kP * KL);
     S.thr_s = reinterpret_cast<float *>(S.Lis + kConsumers * kP * KL);  // [kConsumers][kP]
     S.xv_s = S.thr_s + kConsumers * kP;
@@ -349,14 +366,14 @@ __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL)
     return S;
 }
 
-template <bool BWD>
+template <bool BWD, int ring>
 __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg, const __grid_constant__ CUtensorMap tmD,
                                                                    const __grid_constant__ CUtensorMap tmX)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int K = b.kmax;
-    const int KL = K <= 32 ? 32 : 64;
-    const TmaSmem S = carve_tma(smraw, KL);
+    const int KL = list_slots(K);
+    const TmaSmem S = carve_tma(smraw, KL, ring);
     if (b.st->done) return;
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -369,7 +386,7 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
         S.srcand[threadIdx.x] = b.cands[s < n_cand ? s : 0];
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kRing; ++s) {
+        for (int s = 0; s < ring; ++s) {
             mbar_init(S.full + s, 1);
             mbar_init(S.empty + s, kConsumers);
         }
@@ -392,8 +409,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
             int issued = 0;
             bool ok = true;
             for (int v = 0; v < nvirt; ++v) {
-                const int s = v % kRing;
-                if (!mbar_wait(S.empty + s, ((v / kRing) & 1) ^ 1)) {
+                const int s = v % ring;
+                if (!mbar_wait(S.empty + s, ((v / ring) & 1) ^ 1)) {
                     ok = false;
                     break;
                 }
@@ -410,8 +427,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                 atomicExch(&b.st->error, kErrTimeout);
                 atomicExch(&b.st->done, 1);
                 // drain: wait (bounded) for the copies of the stages still in flight
-                for (int v = issued > kRing ? issued - kRing : 0; v < issued; ++v)
-                    mbar_wait(S.full + v % kRing, (v / kRing) & 1);
+                for (int v = issued > ring ? issued - ring : 0; v < issued; ++v)
+                    mbar_wait(S.full + v % ring, (v / ring) & 1);
             }
         }
         return;
@@ -459,8 +476,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
 #pragma unroll
         for (int p = 0; p < kP; ++p) mn[p] = INFINITY;
         for (int v = 0; v < nA && alive; ++v) {
-            const int s = v % kRing;
-            if (!mbar_wait(S.full + s, (v / kRing) & 1)) {
+            const int s = v % ring;
+            if (!mbar_wait(S.full + s, (v / ring) & 1)) {
                 alive = false;
                 break;
             }
@@ -522,8 +539,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
         };
         load_H();
         for (int v = nA; v < nvirt && alive; ++v) {
-            const int s = v % kRing;
-            if (!mbar_wait(S.full + s, (v / kRing) & 1)) {
+            const int s = v % ring;
+            if (!mbar_wait(S.full + s, (v / ring) & 1)) {
                 alive = false;
                 break;
             }
@@ -533,7 +550,7 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
             const float *D_w = D_s + 2 * lane;
             const float *X_w = X_s + 2 * lane;
             if (wvalid) {
-                const int nch = b.ldc - i0 >= kSC ? kSC / kChunk : 1;  // ldc is a multiple of kChunk
+                const int nch = min(kSC, b.ldc - i0) / kChunk;  // ldc is a multiple of kChunk
 #pragma unroll 1
                 for (int q = 0; q < kSC / kChunk; ++q) {
                     if (q >= nch) break;
@@ -571,8 +588,14 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                             }
                         }
                         if (__any_sync(kFull, pm != 0u)) {
-                            insert_chunk(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K, KL);
-                            load_H();
+                            const unsigned rows = insert_chunk(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K, KL);
+#pragma unroll
+                            for (int ri = 0; ri < kRW; ++ri)
+                                if ((rows >> ri) & 1u) {
+                                    const float h = fmaxf(fmaxf(filter_bound(myT[ri * kCW + 0]), filter_bound(myT[ri * kCW + 1])),
+                                                          fmaxf(filter_bound(myT[ri * kCW + 2]), filter_bound(myT[ri * kCW + 3])));
+                                    H2[ri] = make_float2(h, h);
+                                }
                         }
                     }
                 }
@@ -586,8 +609,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
 #pragma unroll
         for (int p = 0; p < kP; ++p) thr[p] = myT[p];
         for (int v = nA; v < nvirt && alive; ++v) {
-            const int s = v % kRing;
-            if (!mbar_wait(S.full + s, (v / kRing) & 1)) {
+            const int s = v % ring;
+            if (!mbar_wait(S.full + s, (v / ring) & 1)) {
                 alive = false;
                 break;
             }
@@ -670,10 +693,10 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     }
 }
 
-size_t tma_smem_bytes(int K)
+size_t tma_smem_bytes(int K, int ring)
 {
-    const int KL = K <= 32 ? 32 : 64;
-    return sizeof(uint64_t) * 2 * kRing + sizeof(float) * (size_t)kRing * (kRowsB + kCandB) * kSC +
+    const int KL = list_slots(K);
+    return kBarBytes + sizeof(float) * (size_t)ring * (kRowsB + kCandB) * kSC +
            (sizeof(float) + sizeof(int)) * (size_t)kConsumers * kP * KL + 2 * sizeof(float) * kConsumers * kP +
            sizeof(int) * (kCandB + 1);
 }
@@ -724,9 +747,17 @@ cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream
     CUtensorMap tmD, tmX;
     if (!encode_rows(&tmD, b.D, b.ldc, b.n_rows, kRowsB) || !encode_rows(&tmX, b.XT, b.ldc, b.p, 1))
         return cudaErrorInvalidValue;
-    const size_t smem = tma_smem_bytes(b.kmax);
-    auto kern = backward ? k_score_tma<true> : k_score_tma<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // ring depth: as many 32 KB stages as fit beside the lists (16 or 32 slots)
+    int dev = 0, max_smem = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    const bool deep = list_slots(b.kmax) == 16;
+    const size_t smem = tma_smem_bytes(b.kmax, deep ? 6 : 4);
+    if (smem > (size_t)max_smem) return cudaErrorInvalidConfiguration;
+    auto kern = backward ? (deep ? k_score_tma<true, 6> : k_score_tma<true, 4>)
+                         : (deep ? k_score_tma<false, 6> : k_score_tma<false, 4>);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)blocks, (kConsumers + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);
     return cudaGetLastError();

@@ -107,6 +107,8 @@ def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, kernel=0, **kw):
     (999, 333, 12, 9, [3, 30], 4, "forward"),          # k_max 30 -> 4 candidates per thread
     (700, 257, 10, 10, [64], 3, "forward"),            # k_max 64 -> 2 per thread
     (400, 130, 9, 11, [150, 2], 2, "backward"),        # k_max 150 -> 1 per thread
+    (1290, 410, 11, 12, [17, 2], 5, "forward"),        # 32-slot lists; last 256-column stage holds one chunk
+    (830, 300, 10, 13, [20], 6, "backward"),           # backward with 32-slot lists
 ])
 @pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_holdout_matches_oracle(args, kernel):
