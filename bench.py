@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 WORKLOAD = "fwd-64k"
+# DRAM bytes per (validation row, training row) pair of one scoring launch, from an
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum = 549.4 MB for
+# 8192 x 16384 pairs): the D stream read once plus the small X/label traffic.
+TRAFFIC_PER_PAIR = 549.38e6 / (8192 * 16384)
 METRIC = "cand-evals/s (n_val*n_train*candidates per second), greedy forward selection"
 UNIT = "cand-evals/s"
 
@@ -366,12 +370,16 @@ def run_ours(args, world, rank, local):
             "e2e": None if args.no_e2e else {"value": world * evals / e2e_s, "unit": UNIT,
                                              "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp32", "kernel": "k_score", "achieved": achieved_fp32, "peak": fp32_peak,
+            "roofline": {"bound": "fp32", "kernel": "k_score_tma", "achieved": achieved_fp32, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved_fp32 / fp32_peak,
                          "peak_source": f"{sm} SMs x 128 FP32 lanes x {mhz:.0f} MHz (sampled median; no FP32 "
                                         "figure in MEASURED_PEAKS.json); work = 3 rounded FP32 ops per evaluation",
                          "hbm_achieved_gbs": achieved_hbm, "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src,
-                         "hbm_frac": achieved_hbm / hbm, "traffic": args.traffic},
+                         "hbm_frac": achieved_hbm / hbm,
+                         "traffic": args.traffic if args.traffic is not None else TRAFFIC_PER_PAIR * n_val * n_train,
+                         "traffic_source": "command line" if args.traffic is not None else
+                         "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_score_tma launch on the "
+                         "16384 x 8192 case (549.4 MB), scaled per (validation row, training row) pair"},
             "clocks": clocks,
             "result": {"ordering": [int(x) for x in res["ordering"][:steps]],
                        "errors": [float(x) for x in res["errors"][:steps]]}}
