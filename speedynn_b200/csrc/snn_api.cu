@@ -78,6 +78,8 @@ struct snn_handle {
     float *rmse32 = nullptr, *err = nullptr, *stage = nullptr;
     double *rmse64 = nullptr, *err64 = nullptr;
     int *kv = nullptr, *cands = nullptr, *prev_cands = nullptr, *mask = nullptr, *order = nullptr, *stepk = nullptr;
+    int *perm = nullptr;           // candidate slot order: ascending training variance
+    float *fvar = nullptr;         // per-feature training variance
     State *st = nullptr;
     // pruned forward path
     float *Xrow = nullptr;        // training points, row-major
@@ -120,6 +122,7 @@ struct snn_handle {
         b.rmse64 = rmse64;
         b.cands = cands;
         b.prev_cands = prev_cands;
+        b.perm = perm;
         b.mask = mask;
         b.order = order;
         b.err = err;
@@ -154,7 +157,7 @@ void free_all(snn_handle *h)
     cudaSetDevice(h->device);
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors};
+                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : h->score_ev) {
@@ -357,6 +360,8 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->kv, (size_t)h->nk, "k_vals"))) return bail(rc);
     if ((rc = dev_alloc(&h->cands, p, "candidates"))) return bail(rc);
     if ((rc = dev_alloc(&h->prev_cands, p, "candidates"))) return bail(rc);
+    if ((rc = dev_alloc(&h->perm, p, "feature order"))) return bail(rc);
+    if ((rc = dev_alloc(&h->fvar, p, "feature variances"))) return bail(rc);
     if ((rc = dev_alloc(&h->mask, p, "mask"))) return bail(rc);
     if ((rc = dev_alloc(&h->order, p, "ordering"))) return bail(rc);
     if ((rc = dev_alloc(&h->stepk, p, "best k"))) return bail(rc);
@@ -406,6 +411,21 @@ static int load_impl(snn_handle *h, const float *X_train, const float *y_train, 
         if (int rc = load_matrix(h, X_val, h->n_rows, h->XV, h->ldr, device_src)) return rc;
         SNN_CUDA(cudaMemcpyAsync(h->yr, y_val, sizeof(float) * h->n_rows, kind, h->stream));
     }
+    // candidate slot order: ascending training variance, so that the four
+    // candidates a scoring warp shares a filter bound with have distances of
+    // similar scale (any order gives the same results)
+    SNN_CUDA(snn::launch_feature_variance(h->bufs(), h->fvar, h->stream));
+    std::vector<float> var(h->p);
+    SNN_CUDA(cudaMemcpyAsync(var.data(), h->fvar, sizeof(float) * h->p, cudaMemcpyDeviceToHost, h->stream));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<int> perm(h->p);
+    for (int j = 0; j < h->p; ++j) perm[j] = j;
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+        const bool na = std::isnan(var[a]), nb = std::isnan(var[b]);
+        if (na != nb) return nb;  // non-finite columns last
+        return !na && var[a] < var[b];
+    });
+    SNN_CUDA(cudaMemcpyAsync(h->perm, perm.data(), sizeof(int) * h->p, cudaMemcpyHostToDevice, h->stream));
     h->loaded = true;
     reset_timing(h);
     if (int rc = issue_reset(h)) return rc;

@@ -42,8 +42,9 @@ struct Bufs {
     float *pred;
     float *rmse32;
     double *rmse64;
-    int *cands;       // current candidate list (ascending feature ids)
+    int *cands;       // current candidate list, in the order of perm
     int *prev_cands;  // candidate list of the last scored step
+    const int *perm;  // all features, ascending training variance (ties: ascending id)
     int *mask;
     int *order;
     float *err;
@@ -101,6 +102,8 @@ cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s);
 cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_steps, int backward,
                           int auto_feature, cudaStream_t s);
 cudaError_t launch_reset_state(const Bufs &b, int backward, int total_steps, cudaStream_t s);
+// Per-feature training variance (FP64 sums) into var[p], NaN for non-finite columns.
+cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s);
 cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s);
 
 }  // namespace snn

@@ -209,7 +209,8 @@ __global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int
             }
         }
         if (bm < 0) continue;
-        if (best < minv) {
+        // first strict minimum in ascending feature order (slots follow perm)
+        if (best < minv || (best == minv && wi >= 0 && b.cands[ci] < b.cands[wi])) {
             minv = best;
             wi = ci;
             wk = b.kvals[bm];
@@ -233,8 +234,10 @@ __global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int
     st->num_final = backward ? b.p - (t + 1) : t + 1;
     st->step = t + 1;
     int nc = 0;
-    for (int j = 0; j < b.p; ++j)
+    for (int jj = 0; jj < b.p; ++jj) {
+        const int j = b.perm[jj];
         if (b.mask[j] == (backward ? 1 : 0)) b.cands[nc++] = j;
+    }
     st->n_cand = nc;
     if (auto_feature) {
         if (!backward) {
@@ -261,8 +264,10 @@ __global__ void k_force(Bufs b, int w, int it, int t, int total_steps, int backw
     st->num_final = backward ? b.p - (t + 1) : t + 1;
     st->step = t + 1;
     int nc = 0;
-    for (int j = 0; j < b.p; ++j)
+    for (int jj = 0; jj < b.p; ++jj) {
+        const int j = b.perm[jj];
         if (b.mask[j] == (backward ? 1 : 0)) b.cands[nc++] = j;
+    }
     st->n_cand = nc;
     if (t + 1 >= total_steps) st->done = 1;
 }
@@ -276,8 +281,8 @@ __global__ void k_reset_state(Bufs b, int backward, int total_steps)
         b.err[j] = 0.0f;
         b.err64[j] = 0.0;
         b.stepk[j] = 0;
-        b.cands[j] = j;
-        b.prev_cands[j] = j;
+        b.cands[j] = b.perm[j];
+        b.prev_cands[j] = b.perm[j];
     }
     if (j == 0) {
         State s;
@@ -290,6 +295,41 @@ __global__ void k_reset_state(Bufs b, int backward, int total_steps)
         s.num_final = backward ? b.p : 0;
         s.pad = 0;
         *b.st = s;
+    }
+}
+
+// One block per feature: variance of the training column (FP64 sums).  Used
+// only to order candidate slots so that a scoring warp's candidates have
+// distances of similar scale; never part of a result.
+__global__ void k_feature_variance(Bufs b, float *var)
+{
+    const int j = blockIdx.x;
+    const float *x = b.XT + (size_t)j * b.ldc;
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < b.n_cols; i += blockDim.x) {
+        const double v = x[i];
+        s1 += v;
+        s2 += v * v;
+    }
+    __shared__ double r1[8], r2[8];
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        r1[threadIdx.x >> 5] = s1;
+        r2[threadIdx.x >> 5] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t1 = 0.0, t2 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            t1 += r1[w];
+            t2 += r2[w];
+        }
+        const double m = t1 / b.n_cols;
+        const double v = t2 / b.n_cols - m * m;
+        var[j] = isfinite(v) ? (float)fmax(v, 0.0) : NAN;
     }
 }
 
@@ -345,6 +385,12 @@ cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_st
 cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s)
 {
     k_force<<<1, 32, 0, s>>>(b, w, it, t, total_steps, backward);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s)
+{
+    k_feature_variance<<<b.p, 256, 0, s>>>(b, var);
     return cudaGetLastError();
 }
 

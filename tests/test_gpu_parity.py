@@ -194,7 +194,7 @@ def test_headline_shape_subset_rows_against_oracle():
     o = oracle.step(prob, kv, [], list(cands))
     np.testing.assert_array_equal(idx, o["nn_idx"])
     errs = np.array([oracle.rmse32(o["sq32"][ci, 0]) for ci in range(len(cands))])
-    w = int(np.argmin(errs))
+    w = min(range(len(cands)), key=lambda ci: (errs[ci], cands[ci]))  # ties: smallest feature id
     assert r["ordering"][0] == cands[w]
     assert r["errors"][0] == errs[w]
 
