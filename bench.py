@@ -45,11 +45,22 @@ METRIC = "cand-evals/s (n_val*n_train*candidates per second), greedy forward sel
 UNIT = "cand-evals/s"
 
 
-def workload_desc(k, steps, n_train, n_val, p):
-    return {"workload": f"{WORKLOAD}: forward selection, holdout, n_train={n_train}, n_val={n_val}, p={p}, k={k}, "
+def workload_desc(k, steps, n_train, n_val, p, name=WORKLOAD):
+    method = "backward elimination" if name.startswith("bwd") else "forward selection"
+    gb = 4.0 * n_train * n_val / 1e9
+    return {"workload": f"{name}: {method}, holdout, n_train={n_train}, n_val={n_val}, p={p}, k={k}, "
                         f"{steps} greedy steps (seeded synthetic generator)",
             "n_train": n_train, "n_val": n_val, "p": p, "k": k, "greedy_steps": steps,
-            "l2": "inputs larger than L2 (distance matrix 8.6 GB)"}
+            "l2": f"inputs larger than L2 (distance matrix {gb:.1f} GB)"}
+
+
+def scoring_kernel(kmax, option=0):
+    """Name of the full-scan scoring kernel the library picks (option 0 = automatic)."""
+    if option == 3 or (option == 0 and kmax <= 32):
+        return "k_score_tma"
+    if option == 2 or (option == 0 and kmax <= 64):
+        return "k_score_rw"
+    return "k_score"
 
 
 def cand_evals(n_rows, n_cols, p, steps):
@@ -277,8 +288,11 @@ def run_ours(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    w = dict(datagen.WORKLOADS[WORKLOAD])
-    k, steps = w.pop("k"), w.pop("select")
+    name = args.workload
+    w = dict(datagen.WORKLOADS[name])
+    k, select = w.pop("k"), w.pop("select")
+    backward = name.startswith("bwd")
+    steps = w["p"] - select if backward else select  # backward keeps `select` features
     w["seed"] = w["seed"] + 1000 * rank
     if args.rows_scale != 1.0:
         w["n_train"] = int(w["n_train"] * args.rows_scale)
@@ -287,8 +301,9 @@ def run_ours(args, world, rank, local):
     n_train, n_val, p = split.Xtrain.shape[0], split.Xval.shape[0], split.Xtrain.shape[1]
     evals = cand_evals(n_val, n_train, p, steps)
 
-    sel = Selector(split.Xtrain, split.ytrain, split.Xval, split.yval, k_vals=[k], num_features=steps,
-                   method="forward", device=local)
+    sel = Selector(split.Xtrain, split.ytrain, split.Xval, split.yval, k_vals=[k],
+                   num_features=select if backward else steps, method="backward" if backward else "forward",
+                   device=local)
     sel.set_pruning(args.prune)
     sel.set_kernel(args.kernel)
     for _ in range(args.warmup):
@@ -362,7 +377,7 @@ def run_ours(args, world, rank, local):
     line = {"metric": METRIC, "value": world * evals / (ms_step / 1000.0), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(workload_desc(k, steps, n_train, n_val, p), parallelism=f"independent problems x{world}"),
+            "config": dict(workload_desc(k, steps, n_train, n_val, p, name), parallelism=f"independent problems x{world}"),
             "greedy_step_ms": ms_step / steps,
             "breakdown_ms_per_step": {"score": score_ms / args.steps, "commit": commit_ms / args.steps,
                                       "other": (tot_ms - score_ms - commit_ms) / args.steps},
@@ -370,7 +385,8 @@ def run_ours(args, world, rank, local):
             "e2e": None if args.no_e2e else {"value": world * evals / e2e_s, "unit": UNIT,
                                              "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp32", "kernel": "k_score_tma", "achieved": achieved_fp32, "peak": fp32_peak,
+            "roofline": {"bound": "fp32", "kernel": scoring_kernel(k, args.kernel), "achieved": achieved_fp32,
+                         "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved_fp32 / fp32_peak,
                          "peak_source": f"{sm} SMs x 128 FP32 lanes x {mhz:.0f} MHz (sampled median; no FP32 "
                                         "figure in MEASURED_PEAKS.json); work = 3 rounded FP32 ops per evaluation",
@@ -383,7 +399,10 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "result": {"ordering": [int(x) for x in res["ordering"][:steps]],
                        "errors": [float(x) for x in res["errors"][:steps]]}}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if name != WORKLOAD:
+        line["metric"] = METRIC.replace("greedy forward selection", "greedy backward elimination" if backward else
+                                        "greedy forward selection") + f" ({name})"
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and name == WORKLOAD:
         if ref_available():
             rc = RefCPU(split, k, args.cpu_rows)
             e, t = rc.step()
@@ -402,6 +421,55 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_batch(args, world, rank, local):
+    """One bench step = one snn_batch_run over the 320 holdout problems of the
+    batch workload (64 pools x 5 seeded train/validation splits)."""
+    import torch
+
+    from speedynn_b200 import datagen
+    from speedynn_b200.batch import Batch
+
+    torch.cuda.set_device(local)
+    probs = datagen.batch_workload(seed0=4000 + 1000 * rank, scale_rows=args.rows_scale)
+    evals = sum(cand_evals(pr["Xval"].shape[0], pr["Xtrain"].shape[0], pr["Xtrain"].shape[1], pr["num_features"])
+                for pr in probs)
+    d_bytes = sum(4.0 * pr["Xval"].shape[0] * pr["Xtrain"].shape[0] for pr in probs)
+    b = Batch(probs)
+    for _ in range(args.warmup):
+        b.run()
+    clk = Clocks(local)
+    clk.start()
+    run_ms = 0.0
+    wall = 0.0
+    waves = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        b.run()
+        wall += time.perf_counter() - t0
+        tm = b.timing()
+        run_ms += tm["run_ms"]
+        waves = tm["waves"]
+    clocks = clk.stop()
+    b.close()
+    ms = run_ms / args.steps
+    h2d = sum(pr["Xtrain"].nbytes + pr["ytrain"].nbytes + pr["Xval"].nbytes + pr["yval"].nbytes for pr in probs)
+    n_tr = [pr["Xtrain"].shape[0] for pr in probs]
+    line = {"metric": METRIC + " (batch-64x5)", "value": world * evals / (ms / 1000.0), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batch-64x5: {len(probs)} holdout forward selections (64 pools, n_train "
+                                   f"log-uniform in [1024, 40000] -> {min(n_tr)}..{max(n_tr)}, n_val = n_train/2, "
+                                   f"p=40, k in {{1,5,10,20}}, 15 steps, 5 seeded splits each)",
+                       "problems": len(probs), "distance_matrices_gb": d_bytes / 1e9, "waves": waves,
+                       "l2": "inputs larger than L2", "parallelism": "one CUDA stream per problem"},
+            "e2e": {"value": world * evals / (wall / args.steps), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(sum(pr["Xtrain"].shape[1] * 28 + 8 for pr in probs))},
+            "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,12 +484,18 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiler captures)")
     ap.add_argument("--prune", type=int, default=0, help="exact pruning of forward steps (library option)")
     ap.add_argument("--kernel", type=int, default=0, help="full-scan kernel: 0 auto, 1 rows per lane, 2 row per warp")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=["fwd-64k", "bwd-50k", "fwd-200k", "batch-64x5"],
+                    help="fwd-64k (the headline), bwd-50k (backward, p=120 -> 20), fwd-200k (80 GB distance matrix, "
+                         "k=50), batch-64x5 (320 holdout problems in one batch)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per scoring launch, scaled to this workload (reported as roofline.traffic)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload.startswith("batch"):
+        return run_batch(args, world, rank, local)
     return run_ours(args, world, rank, local)
 
 

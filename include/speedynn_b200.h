@@ -145,8 +145,8 @@ SNN_API int snn_get_results(snn_handle *h, int *ordering, int *mask, float *erro
 
 /* Neighbour lists of the most recent step, for inspection: when enabled
  * before a step, that step keeps idx/dist[n_cand][n_rows][k_max] (candidates
- * in ascending feature order, listed in cands[n_cand]).  Pass NULL to query
- * sizes through n_cand/k_max. */
+ * in the handle's slot order -- ascending training variance -- listed in
+ * cands[n_cand]).  Pass NULL to query sizes through n_cand/k_max. */
 SNN_API int snn_keep_neighbours(snn_handle *h, int enable);
 SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_max, int *idx, float *dist);
 
@@ -176,6 +176,45 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value);
 SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, unsigned long long *pairs_survived);
 
 SNN_API int snn_destroy(snn_handle *h);
+
+/* ---------------------------------------------------------------------------
+ * 2b. Batches of independent problems
+ *
+ * No single reference function: the reference runs one problem per process
+ * (global state, speedynn/lib/nearest_neighbors_feature_selection.c:6-35).
+ * A batch runs many selections -- different shapes, k values, directions --
+ * with each problem on its own CUDA stream so small problems overlap on the
+ * GPU.  Problems are grouped into waves that fit the device memory budget
+ * (max_device_bytes, or 0 for the free memory less a reserve); each wave's
+ * handles are created, loaded, run and freed in turn.  Results are those of
+ * snn_create/snn_load/snn_run on each problem alone.
+ * ------------------------------------------------------------------------- */
+
+typedef struct snn_batch snn_batch;
+
+/* Copy and validate n descriptors (k_vals are copied); no device memory yet. */
+SNN_API int snn_batch_create(const snn_desc *descs, int n, unsigned long long max_device_bytes, snn_batch **out);
+
+/* Attach problem i's host inputs (row-major float32, as snn_load).  The
+ * arrays are read during snn_batch_run and must stay valid until it returns. */
+SNN_API int snn_batch_load(snn_batch *b, int i, const float *X_train, const float *y_train, const float *X_val,
+                           const float *y_val);
+
+/* Run every problem's whole selection; blocks until all are done.  A failing
+ * problem keeps its status for snn_batch_get_results; device or argument
+ * errors stop the batch with a negative status. */
+SNN_API int snn_batch_run(snn_batch *b);
+
+/* Problem i's results, as snn_get_results; returns that problem's status. */
+SNN_API int snn_batch_get_results(snn_batch *b, int i, int *ordering, int *mask, float *errors, double *errors64,
+                                  int *step_best_k, int *best_k, int *num_final);
+
+/* Wall time of the last snn_batch_run spent running waves (from the first
+ * launch of a wave to its last result; creating and loading excluded), and
+ * the number of waves. */
+SNN_API int snn_batch_get_timing(snn_batch *b, double *run_ms, int *waves);
+
+SNN_API int snn_batch_destroy(snn_batch *b);
 
 /* ---------------------------------------------------------------------------
  * 3. One greedy step without device allocation

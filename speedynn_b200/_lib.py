@@ -74,6 +74,14 @@ def lib():
             "snn_destroy": (ctypes.c_int, [vp]),
             "snn_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "snn_get_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]),
+            "snn_batch_create": (ctypes.c_int, [ctypes.POINTER(SnnDesc), ctypes.c_int, ctypes.c_ulonglong,
+                                                ctypes.POINTER(vp)]),
+            "snn_batch_load": (ctypes.c_int, [vp, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]),
+            "snn_batch_run": (ctypes.c_int, [vp]),
+            "snn_batch_get_results": (ctypes.c_int, [vp, ctypes.c_int, _i32p, _i32p, _f32p, _f64p, _i32p, _i32p,
+                                                     _i32p]),
+            "snn_batch_get_timing": (ctypes.c_int, [vp, _f64p, _i32p]),
+            "snn_batch_destroy": (ctypes.c_int, [vp]),
             "snn_last_error": (ctypes.c_char_p, []),
             "snn_version": (ctypes.c_char_p, []),
             "train_forward_selection": (ctypes.c_int, [_f32p, ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int, _i32p,

@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -286,11 +287,9 @@ SNN_API const char *snn_last_error(void) { return g_err.c_str(); }
 
 SNN_API const char *snn_version(void) { return "speedynn_b200 0.1.0 (sm_100a)"; }
 
-SNN_API int snn_create(const snn_desc *d, snn_handle **out)
+// Descriptor checks shared by snn_create and snn_batch_create (no CUDA calls).
+static int validate_desc(const snn_desc *d, int *kmax_out)
 {
-    g_err.clear();
-    if (!d || !out) return fail(SNN_ERR_ARG, "null descriptor or output pointer");
-    *out = nullptr;
     if (d->n_train <= 0 || d->p <= 0 || d->n_val < 0) return fail(SNN_ERR_ARG, "bad shape n_train=%d n_val=%d p=%d",
                                                                  d->n_train, d->n_val, d->p);
     if (!d->k_vals || d->num_k_vals <= 0) return fail(SNN_ERR_ARG, "k_vals must be a non-empty array");
@@ -301,9 +300,38 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     }
     if (d->num_features < 0 || d->num_features > d->p)
         return fail(SNN_ERR_ARG, "num_features=%d must lie in [0, p=%d]", d->num_features, d->p);
-    const int cv = d->n_val == 0;
-    if (cv && (d->k_fold <= 0 || d->k_fold > d->n_train))
+    if (d->n_val == 0 && (d->k_fold <= 0 || d->k_fold > d->n_train))
         return fail(SNN_ERR_ARG, "k_fold=%d must lie in [1, n=%d]", d->k_fold, d->n_train);
+    if (kmax > snn::kScoreMaxK)
+        return fail(SNN_ERR_UNSUPPORTED, "k_max=%d is above the supported maximum of %d", kmax, snn::kScoreMaxK);
+    *kmax_out = kmax;
+    return SNN_OK;
+}
+
+// Device bytes a handle for this descriptor allocates (buffers of snn_create
+// plus the load staging buffer), for the batch's memory waves.
+static size_t handle_bytes(const snn_desc *d, int kmax)
+{
+    const size_t p = (size_t)d->p, n_cols = (size_t)d->n_train;
+    const bool cv = d->n_val == 0;
+    const size_t n_rows = cv ? n_cols : (size_t)d->n_val;
+    const size_t ldc = (size_t)round_up(d->n_train, snn::kPadCols);
+    const size_t ldr = cv ? ldc : (size_t)round_up((int)n_rows, snn::kPadCols);
+    const size_t M = d->backward ? 0 : (size_t)snn::seeds_for_k(kmax);
+    size_t f = p * ldc + n_rows * ldc + p * (size_t)d->num_k_vals * n_rows + p * n_cols + std::max(n_rows, n_cols) * p +
+               n_rows * M + n_cols + n_rows;
+    if (!cv) f += p * ldr;
+    return sizeof(float) * f + ((size_t)1 << 20);
+}
+
+SNN_API int snn_create(const snn_desc *d, snn_handle **out)
+{
+    g_err.clear();
+    if (!d || !out) return fail(SNN_ERR_ARG, "null descriptor or output pointer");
+    *out = nullptr;
+    int kmax = 0;
+    if (int rc = validate_desc(d, &kmax)) return rc;
+    const int cv = d->n_val == 0;
     if (int rc = check_device(d->device)) return rc;
 
     snn_handle *h = new snn_handle();
@@ -640,6 +668,193 @@ SNN_API int snn_destroy(snn_handle *h)
     if (!h) return SNN_OK;
     free_all(h);
     delete h;
+    return SNN_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batches of independent problems
+// ===========================================================================
+struct snn_batch {
+    struct Problem {
+        snn_desc desc;
+        std::vector<int> kvals;
+        const float *Xt = nullptr, *yt = nullptr, *Xv = nullptr, *yv = nullptr;
+        int status = SNN_ERR_STATE;  // until run
+        std::vector<int> ordering, mask, stepk;
+        std::vector<float> err;
+        std::vector<double> err64;
+        int best_k = 0, num_final = 0;
+    };
+    std::vector<Problem> prob;
+    unsigned long long max_bytes = 0;  // 0: free device memory less a reserve
+    double run_ms = 0.0;
+    int waves = 0;
+};
+
+namespace {
+
+// Run problems [i0, i1) of the batch, all created and loaded: every selection
+// is issued on its handle's own stream before any result is read, so the
+// problems overlap on the GPU.
+int run_wave(snn_batch *B, std::vector<snn_handle *> &hs, int i0)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    for (snn_handle *h : hs) {
+        if (cudaSetDevice(h->device) != cudaSuccess) return fail(SNN_ERR_CUDA, "cudaSetDevice failed");
+        reset_timing(h);
+        if (int rc = issue_reset(h)) return rc;
+        for (int t = 0; t < h->total_steps; ++t)
+            if (int rc = issue_step(h, t)) return rc;
+        h->host_step = h->total_steps;
+    }
+    for (size_t j = 0; j < hs.size(); ++j) {
+        snn_handle *h = hs[j];
+        snn_batch::Problem &P = B->prob[i0 + j];
+        State st;
+        cudaSetDevice(h->device);
+        if (int rc = read_state(h, &st)) return rc;
+        const size_t p = (size_t)h->p;
+        P.ordering.assign(p, 0);
+        P.mask.assign(p, 0);
+        P.stepk.assign(p, 0);
+        P.err.assign(p, 0.0f);
+        P.err64.assign(p, 0.0);
+        P.status = st.error == snn::kErrTimeout ? SNN_ERR_TIMEOUT : st.error;
+        if (int rc = snn_get_results(h, P.ordering.data(), P.mask.data(), P.err.data(), P.err64.data(), P.stepk.data(),
+                                     &P.best_k, &P.num_final))
+            P.status = rc;
+    }
+    B->run_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    B->waves++;
+    return SNN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+SNN_API int snn_batch_create(const snn_desc *descs, int n, unsigned long long max_device_bytes, snn_batch **out)
+{
+    g_err.clear();
+    if (!descs || !out || n <= 0) return fail(SNN_ERR_ARG, "snn_batch_create needs n >= 1 descriptors and an output");
+    *out = nullptr;
+    snn_batch *B = new snn_batch();
+    B->prob.resize(n);
+    for (int i = 0; i < n; ++i) {
+        int kmax = 0;
+        if (int rc = validate_desc(descs + i, &kmax)) {
+            delete B;
+            return fail(rc, "problem %d: %s", i, std::string(g_err).c_str());
+        }
+        B->prob[i].desc = descs[i];
+        B->prob[i].kvals.assign(descs[i].k_vals, descs[i].k_vals + descs[i].num_k_vals);
+        B->prob[i].desc.k_vals = B->prob[i].kvals.data();
+    }
+    B->max_bytes = max_device_bytes;
+    *out = B;
+    return SNN_OK;
+}
+
+SNN_API int snn_batch_load(snn_batch *B, int i, const float *X_train, const float *y_train, const float *X_val,
+                           const float *y_val)
+{
+    g_err.clear();
+    if (!B || i < 0 || i >= (int)B->prob.size()) return fail(SNN_ERR_ARG, "snn_batch_load: no problem %d", i);
+    snn_batch::Problem &P = B->prob[i];
+    if (!X_train || !y_train) return fail(SNN_ERR_ARG, "X_train and y_train are required");
+    if (P.desc.n_val > 0 && (!X_val || !y_val)) return fail(SNN_ERR_ARG, "holdout mode needs X_val and y_val");
+    P.Xt = X_train;
+    P.yt = y_train;
+    P.Xv = X_val;
+    P.yv = y_val;
+    return SNN_OK;
+}
+
+SNN_API int snn_batch_run(snn_batch *B)
+{
+    g_err.clear();
+    if (!B) return fail(SNN_ERR_ARG, "null batch");
+    for (size_t i = 0; i < B->prob.size(); ++i)
+        if (!B->prob[i].Xt) return fail(SNN_ERR_STATE, "snn_batch_run: problem %zu has no inputs", i);
+    B->run_ms = 0.0;
+    B->waves = 0;
+    const int n = (int)B->prob.size();
+    int i = 0;
+    while (i < n) {
+        // one wave: consecutive problems on one device within the memory budget
+        const int dev = B->prob[i].desc.device;
+        if (int rc = check_device(dev)) return rc;
+        SNN_CUDA(cudaSetDevice(dev));
+        size_t budget = (size_t)B->max_bytes;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            SNN_CUDA(cudaMemGetInfo(&fr, &tot));
+            const size_t reserve = std::max<size_t>((size_t)1 << 30, tot / 50);
+            budget = fr > reserve ? fr - reserve : 0;
+        }
+        std::vector<snn_handle *> hs;
+        size_t used = 0;
+        const int i0 = i;
+        int rc = SNN_OK;
+        while (i < n && B->prob[i].desc.device == dev) {
+            int kmax = 0;
+            validate_desc(&B->prob[i].desc, &kmax);
+            const size_t need = handle_bytes(&B->prob[i].desc, kmax);
+            if (!hs.empty() && used + need > budget) break;
+            snn_handle *h = nullptr;
+            const snn_batch::Problem &P = B->prob[i];
+            if ((rc = snn_create(&P.desc, &h)) || (rc = snn_load(h, P.Xt, P.yt, P.Xv, P.yv))) {
+                snn_destroy(h);
+                if (rc == SNN_ERR_NOMEM && !hs.empty()) {
+                    rc = SNN_OK;  // run what fits, retry this problem in the next wave
+                    break;
+                }
+                break;
+            }
+            hs.push_back(h);
+            used += need;
+            ++i;
+        }
+        if (rc == SNN_OK && !hs.empty()) rc = run_wave(B, hs, i0);
+        for (snn_handle *h : hs) snn_destroy(h);
+        if (rc) return fail(rc, "snn_batch_run, problem %d: %s", i, std::string(g_err).c_str());
+    }
+    return SNN_OK;
+}
+
+SNN_API int snn_batch_get_results(snn_batch *B, int i, int *ordering, int *mask, float *errors, double *errors64,
+                                  int *step_best_k, int *best_k, int *num_final)
+{
+    g_err.clear();
+    if (!B || i < 0 || i >= (int)B->prob.size()) return fail(SNN_ERR_ARG, "snn_batch_get_results: no problem %d", i);
+    const snn_batch::Problem &P = B->prob[i];
+    if (P.status == SNN_ERR_STATE && P.ordering.empty()) return fail(SNN_ERR_STATE, "problem %d has not run", i);
+    const size_t p = (size_t)P.desc.p;
+    if (ordering) memcpy(ordering, P.ordering.data(), sizeof(int) * p);
+    if (mask) memcpy(mask, P.mask.data(), sizeof(int) * p);
+    if (errors) memcpy(errors, P.err.data(), sizeof(float) * p);
+    if (errors64) memcpy(errors64, P.err64.data(), sizeof(double) * p);
+    if (step_best_k) memcpy(step_best_k, P.stepk.data(), sizeof(int) * p);
+    if (best_k) *best_k = P.best_k;
+    if (num_final) *num_final = P.num_final;
+    if (P.status) return fail(P.status, "problem %d ended with status %d", i, P.status);
+    return SNN_OK;
+}
+
+SNN_API int snn_batch_get_timing(snn_batch *B, double *run_ms, int *waves)
+{
+    g_err.clear();
+    if (!B) return fail(SNN_ERR_ARG, "null batch");
+    if (run_ms) *run_ms = B->run_ms;
+    if (waves) *waves = B->waves;
+    return SNN_OK;
+}
+
+SNN_API int snn_batch_destroy(snn_batch *B)
+{
+    delete B;
     return SNN_OK;
 }
 

@@ -103,3 +103,28 @@ def workload(name, scale_rows=1.0):
     w["n_train"] = max(64, int(w["n_train"] * scale_rows))
     w["n_val"] = max(32, int(w["n_val"] * scale_rows))
     return generate(**w), k, sel
+
+
+def batch_workload(seed0=4000, n_pools=64, n_splits=5, p=40, lo=1024, hi=40000, steps=15, scale_rows=1.0):
+    """The batched workload: ``n_pools`` problems with n_train log-uniform in
+    [lo, hi] (seeded per pool: seed0 + i), a pool of 1.5 * n_train rows each,
+    and ``n_splits`` seeded train / validation splits of every pool (n_val =
+    n_train / 2), so n_pools * n_splits holdout forward selections; pool i uses
+    k = (1, 5, 10, 20)[i % 4] and ``steps`` greedy steps.  Returns a list of
+    problem dicts for :class:`speedynn_b200.batch.Batch`."""
+    probs = []
+    for i in range(n_pools):
+        rng = np.random.default_rng(seed0 + i)
+        n = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))) * scale_rows))
+        n = max(64, n)
+        pool = generate(n, n // 2, p, n_mag=6, seed=seed0 + i)
+        X = np.concatenate([pool.Xtrain, pool.Xval])
+        y = np.concatenate([pool.ytrain, pool.yval])
+        k = (1, 5, 10, 20)[i % 4]
+        for s in range(n_splits):
+            perm = np.random.default_rng((seed0 + i) * 31 + s).permutation(X.shape[0])
+            tr, va = perm[:n], perm[n:n + n // 2]
+            probs.append(dict(Xtrain=np.ascontiguousarray(X[tr]), ytrain=np.ascontiguousarray(y[tr]),
+                              Xval=np.ascontiguousarray(X[va]), yval=np.ascontiguousarray(y[va]), k_vals=[k],
+                              num_features=steps, method="forward"))
+    return probs

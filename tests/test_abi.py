@@ -120,3 +120,18 @@ def test_no_gpu_means_error_not_fallback(L):
         pytest.skip("a usable GPU is visible")
     assert rc == _lib.SNN_ERR_CUDA
     assert b"device" in L.snn_last_error() or b"CUDA" in L.snn_last_error()
+
+
+def test_batch_rejects_bad_descriptors_without_a_gpu():
+    """snn_batch_create validates every descriptor before touching a device."""
+    import numpy as np
+    from speedynn_b200 import _lib
+    from speedynn_b200.batch import Batch
+    good = dict(Xtrain=np.zeros((50, 4), np.float32), ytrain=np.zeros(50, np.float32), k_vals=[3], num_features=2,
+                k_fold=5)
+    bad = dict(good, k_vals=[0])
+    with pytest.raises(Exception) as e:
+        Batch([good, bad])
+    assert "problem 1" in str(e.value)
+    L = _lib.lib()
+    assert L.snn_batch_create(None, 0, 0, None) == _lib.SNN_ERR_ARG

@@ -1,0 +1,48 @@
+"""Batches (snn_batch_*): each problem's results equal a Selector run of
+that problem alone -- bit for bit, as the batch reuses the same handles --
+whether the batch runs in one wave or in one wave per problem."""
+import numpy as np
+import pytest
+
+from speedynn_b200 import datagen
+from speedynn_b200.batch import Batch
+from speedynn_b200.selector import Selector
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("ordering", "mask", "errors", "errors64", "step_best_k", "best_k", "num_final")
+
+
+def _problems():
+    probs = []
+    shapes = [(1500, 700, 12, [10], 4, "forward"), (900, 0, 10, [1, 5], 3, "forward"),
+              (1200, 500, 14, [5, 20], 9, "backward"), (700, 300, 9, [3], 5, "forward"),
+              (2100, 0, 11, [7, 2], 6, "backward"), (1000, 450, 13, [40], 3, "forward")]
+    for i, (nt, nv, p, kv, nf, method) in enumerate(shapes):
+        s = datagen.generate(nt, max(nv, 32), p, n_mag=5, seed=500 + i)
+        pr = dict(Xtrain=s.Xtrain, ytrain=s.ytrain, k_vals=kv, num_features=nf, method=method, k_fold=4)
+        if nv:
+            pr.update(Xval=s.Xval, yval=s.yval)
+        probs.append(pr)
+    probs[3]["auto_feature"] = True
+    return probs
+
+
+def _alone(pr):
+    kw = {k: v for k, v in pr.items() if k not in ("Xtrain", "ytrain", "Xval", "yval")}
+    with Selector(pr["Xtrain"], pr["ytrain"], pr.get("Xval"), pr.get("yval"), **kw) as sel:
+        return sel.run()
+
+
+@pytest.mark.parametrize("max_bytes", [0, 1])
+def test_batch_matches_single_runs(max_bytes):
+    probs = _problems()
+    want = [_alone(pr) for pr in probs]
+    with Batch(probs, max_device_bytes=max_bytes) as b:
+        got = b.run()
+        tm = b.timing()
+    assert tm["waves"] == (1 if max_bytes == 0 else len(probs))
+    assert tm["run_ms"] > 0
+    for w, g in zip(want, got):
+        for k in KEYS:
+            np.testing.assert_array_equal(np.asarray(g[k]), np.asarray(w[k]), err_msg=k)
