@@ -229,3 +229,26 @@ def test_pruned_forward_equals_full_scan(args):
         np.testing.assert_array_equal(a, b)
     assert ca["pairs_streamed"] > 0 and ca["pairs_survived"] < ca["pairs_streamed"]
     assert cb["pairs_streamed"] == 0
+
+
+@pytest.mark.parametrize("kv", [[10], [50, 7]])
+def test_large_problem_sampled_rows_match_oracle(kv):
+    """At a size the oracle cannot hold whole (120,000 training x 30,000
+    validation rows, mixture features, 2 % duplicated training rows): after
+    three committed steps, the fourth step's neighbour lists of 96 sampled
+    validation rows equal the oracle's, which recomputes those rows'
+    distances from X in commit order.  k = 10 runs the TMA-fed kernel,
+    k = 50 the row-tile kernel."""
+    s = datagen.generate(120000, 30000, 24, n_mag=8, seed=55, mixture=True, dup_frac=0.02)
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=kv, num_features=4, method="forward") as sel:
+        for _ in range(3):
+            assert sel.step()
+        committed = [int(c) for c in sel.results()["ordering"][:3]]
+        sel.keep_neighbours(True)
+        assert sel.step()
+        cands, idx, dist = sel.neighbours()
+    rows = np.sort(np.random.default_rng(5).choice(s.Xval.shape[0], 96, replace=False)).astype(np.int32)
+    prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
+    o = oracle.step(prob, kv, committed, list(cands), rows=rows)
+    np.testing.assert_array_equal(idx[:, rows], o["nn_idx"])
+    np.testing.assert_array_equal(dist[:, rows], o["nn_dist"])
