@@ -236,8 +236,11 @@ SNN_API int snn_batch_destroy(snn_batch *b);
  * excluded pairs); XT [p][ld] training points feature-major; XV [p][ldr]
  * scored points feature-major; y_train [n_train], y_val [n_rows].  cands
  * and k_vals are HOST arrays (feature ids to score, k values).  backward=1
- * scores removals (D - square) instead of additions.  stream: a
- * cudaStream_t (NULL = legacy default stream); the call waits for it.
+ * scores removals (D - square) instead of additions.  D and XT must be
+ * 16-byte aligned (they are read with TMA copies).  For a forward step
+ * (backward=0) every entry of D must be >= 0 or +inf, as sums of squares
+ * are: the scorer's exact filter relies on it.  stream: a cudaStream_t
+ * (NULL = legacy default stream); the call waits for it.
  *
  * The first call on each device looks up the scratch's device address
  * (with that device current); make that first call before any stream
