@@ -2,13 +2,15 @@
 //
 // Contract as snn_score_rw.cu: exact top-k_max lists (k <= 32) in the
 // reference's stable (distance, index) order and kNN-mean predictions.  A
-// block scores 16 rows x 16 candidates; each of its 16 consumer warps owns 4
-// rows x 4 candidates and walks the columns two per lane with packed f32x2.
+// block scores 24 rows x 12 candidates; each of its 18 consumer warps owns 4
+// rows x 4 candidates and walks the columns two per lane with packed f32x2
+// (18 consumers + 1 producer = 19 warps, at most 5 per SM sub-partition at
+// 96 registers; 12-candidate groups leave no padded slot for 60 candidates).
 //
 //   * Feed: one producer lane streams 256-column stages into a ring of
-//     shared-memory slots (as deep as fits beside the lists, at most 8): a
-//     2-D tensor-map TMA copy of the 16 D rows and four tile::gather4 copies
-//     of the 16 candidate rows of X, all completing on the stage's "full"
+//     shared-memory slots (as deep as fits beside the lists): a 2-D
+//     tensor-map TMA copy of the 24 D rows and three tile::gather4 copies
+//     of the 12 candidate rows of X, all completing on the stage's "full"
 //     mbarrier; consumers release a slot through its "empty" mbarrier, so a
 //     warp busy inserting falls behind by up to a ring of stages without
 //     stalling the others.
@@ -42,9 +44,11 @@ constexpr int kSC = 256;          // columns per stage
 constexpr int kMaxRing = 8;       // most stages in the ring (the depth is a template argument)
 constexpr int kBarBytes = 128;    // full + empty mbarriers, padded so the tiles stay 128-byte aligned
 static_assert(2 * kMaxRing * sizeof(uint64_t) <= kBarBytes, "mbarriers must fit their area");
-constexpr int kRowsB = 16;        // scored rows per block
-constexpr int kCandB = 16;        // candidates per block
-constexpr int kConsumers = 16;    // consumer warps (4 row groups x 4 candidate groups)
+constexpr int kRowsB = 24;        // scored rows per block
+constexpr int kCandB = 12;        // candidates per block
+constexpr int kConsumers = 18;    // consumer warps (6 row groups x 3 candidate groups)
+constexpr int kRingDeep = 5;      // ring slots beside 16-slot lists (k <= 16)
+constexpr int kRingShallow = 4;   // ring slots beside 32-slot lists (k <= 32)
 constexpr int kRW = 4, kCW = 4, kP = kRW * kCW;
 constexpr long long kSpinLimit = 1ll << 22;  // try_wait polls before giving up
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one second
@@ -753,10 +757,10 @@ cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     const bool deep = list_slots(b.kmax) == 16;
-    const size_t smem = tma_smem_bytes(b.kmax, deep ? 6 : 4);
+    const size_t smem = tma_smem_bytes(b.kmax, deep ? kRingDeep : kRingShallow);
     if (smem > (size_t)max_smem) return cudaErrorInvalidConfiguration;
-    auto kern = backward ? (deep ? k_score_tma<true, 6> : k_score_tma<true, 4>)
-                         : (deep ? k_score_tma<false, 6> : k_score_tma<false, 4>);
+    auto kern = backward ? (deep ? k_score_tma<true, kRingDeep> : k_score_tma<true, kRingShallow>)
+                         : (deep ? k_score_tma<false, kRingDeep> : k_score_tma<false, kRingShallow>);
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)blocks, (kConsumers + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);
