@@ -49,6 +49,14 @@ extern "C" {
 
 /* loss ids, speedynn/base.py:13-23 */
 #define SNN_LOSS_RMSE 0
+#define SNN_LOSS_RMSE_NORM 1
+#define SNN_LOSS_MAD 2
+#define SNN_LOSS_MAD_NORM 3
+#define SNN_LOSS_ZERO_ONE 4
+#define SNN_LOSS_STD 5
+#define SNN_LOSS_RMSE_NORM_MAD_NORM_STD 6
+#define SNN_LOSS_RMSE_NORM_MAD_NORM_GALAXIES 7
+#define SNN_LOSS_RMSE_STD 8
 
 /* ---------------------------------------------------------------------------
  * 1. Reference-compatible entry points
@@ -58,8 +66,8 @@ extern "C" {
  * (speedynn/lib/nearest_neighbors_feature_selection.h:65, .c:60-65).
  * CV mode over Xtrain [nXtrain][dXtrain]: folds are contiguous row blocks of
  * nXtrain / kfold rows (a remainder forms an extra fold).  Returns the final
- * number of features, or a negative status.  loss_functions[0] must be
- * SNN_LOSS_RMSE; model_type must be 0 (regression). */
+ * number of features, or a negative status.  loss_functions: reference
+ * loss ids, the first decides; model_type 0 regression, 1 classification. */
 SNN_API int train_forward_selection(float *Xtrain, int nXtrain, int dXtrain, float *Ytrain, int nYtrain,
                                     int *kvals, int num_kvals, int num_features, int kfold,
                                     int *loss_functions, int num_loss_functions, int auto_feature,
@@ -142,6 +150,23 @@ SNN_API int snn_commit_sequence(snn_handle *h, const int *seq, int n);
  * residuals summed in FP64; step_best_k: best k of each step's winner. */
 SNN_API int snn_get_results(snn_handle *h, int *ordering, int *mask, float *errors, double *errors64,
                             int *step_best_k, int *best_k, int *num_final);
+
+/* Model and losses (speedynn/lib/cpu.c:21-126, loss_functions.c:6-183).
+ * model_type 0 predicts the mean of the k nearest labels, 1 (classification)
+ * their mode with the reference's rule (first position of the strictly
+ * largest count, each label counted at its first occurrence in rank order,
+ * util.c:165-188).  Every loss of loss_ids (reference ids 0..8, the
+ * SNN_LOSS_* values) is evaluated for every candidate and k with the
+ * reference's float/double operation order; loss_ids[0] picks each
+ * candidate's best k and the winner, and snn_get_errors_all returns all of
+ * them for each step's winner.  When loss_ids[0] is not RMSE, errors64 of
+ * snn_get_results holds that loss's FP32 value.  Default: {RMSE},
+ * regression.  Resets a loaded handle to step 0. */
+SNN_API int snn_set_model(snn_handle *h, const int *loss_ids, int n_losses, int model_type);
+
+/* Every loss of every step, in the reference's selected_errors layout
+ * errors[l * p + i] (n >= n_losses * p). */
+SNN_API int snn_get_errors_all(snn_handle *h, float *errors, int n);
 
 /* Neighbour lists of the most recent step, for inspection: when enabled
  * before a step, that step keeps idx/dist[n_cand][n_rows][k_max] (candidates

@@ -142,9 +142,82 @@ def rmse32(sq):
 # of (distance, index) restricted to distance < FLT_MAX, padded with
 # (FLT_MAX, 0) (speedynn/lib/cpu.c:212-252).
 # --------------------------------------------------------------------------
-def np_select(prob, k_vals, num_features, method="forward"):
+def np_loss(labels, preds, lid):
+    """speedynn/lib/loss_functions.c:6-183 with the reference's float/double
+    operation order (sequential FP32 sums, double divisions where C promotes)."""
+    y = np.asarray(labels, np.float32)
+    pr = np.asarray(preds, np.float32)
+    n = y.size
+    f32, f64 = np.float32, np.float64
+
+    def rmse():
+        e = y - pr
+        return rmse32(e * e)
+
+    def rmse_norm():  # :52-62, descending index order
+        tmp = ((y - pr).astype(f64) / (1.0 + y.astype(f64))).astype(f32)
+        s = np.add.accumulate((tmp * tmp)[::-1], dtype=f32)[-1]
+        return f32(np.sqrt(f64(f32(s / f32(n)))))
+
+    def mad(norm):  # :66-111, find_median = sorted[n / 2] (:173-183)
+        e = ((y - pr).astype(f64) / (1.0 + y.astype(f64))).astype(f32) if norm else (y - pr)
+        m1 = np.sort(e)[n // 2]
+        return np.sort(np.abs(e - m1))[n // 2]
+
+    def zero_one():  # :113-127, int abs() of the truncated difference
+        a = np.abs(y - pr)
+        miss = np.count_nonzero((a >= 1.0) & (a < 2147483648.0))
+        return f32(f32(miss) / f32(n))
+
+    def std():  # :129-143, the loop assigns: only the last row's term remains
+        mean = np.add.accumulate(y - pr, dtype=f32)[-1]
+        mean = f32(mean / f32(n))
+        a = f32(f32(y[-1] - pr[-1]) - mean)
+        return f32(np.sqrt(f64(f32(f32(a * a) / f32(n - 1)))))
+
+    if lid == 0:
+        return rmse()
+    if lid == 1:
+        return rmse_norm()
+    if lid == 2:
+        return mad(False)
+    if lid == 3:
+        return mad(True)
+    if lid == 4:
+        return zero_one()
+    if lid == 5:
+        return std()
+    if lid == 6:
+        return f32(f64(rmse_norm()) / 0.19 + f64(mad(True)) / 0.041 + f64(std()) / 0.16)
+    if lid == 7:
+        return f32(f64(rmse_norm()) / 0.019 + f64(mad(True)) / 0.009)
+    if lid == 8:
+        return f32(rmse() + std())
+    raise ValueError(lid)
+
+
+def np_mode(labels):
+    """speedynn/lib/util.c:165-188: each label counts at its first occurrence;
+    the first position with the strictly largest count wins."""
+    k = len(labels)
+    rep = np.zeros(k, np.int64)
+    for i in range(k):
+        j = 0
+        while j < i and labels[i] != labels[j]:
+            j += 1
+        rep[j] += 1
+    best = 0
+    for i in range(1, k):
+        if rep[i] > rep[best]:
+            best = i
+    return labels[best]
+
+
+def np_select(prob, k_vals, num_features, method="forward", loss_functions=(0,), model_type=0, auto_feature=False):
     kv = np.asarray(k_vals, np.int32)
     kmax = int(kv.max())
+    lids = [int(x) for x in loss_functions]
+    nl = len(lids)
     Xr, Xc, yr, yc = prob.Xr, prob.Xc, prob.yr, prob.yc
     nr, nc, p = Xr.shape[0], Xc.shape[0], prob.p
     back = method == "backward"
@@ -165,14 +238,16 @@ def np_select(prob, k_vals, num_features, method="forward"):
     mask = np.ones(p, np.int32) if back else np.zeros(p, np.int32)
     ordering = np.zeros(p, np.int32)
     errors = np.zeros(p, np.float32)
+    errors_all = np.zeros((nl, p), np.float32)
     best_k_last = 0
-    its = range(p - 1, num_features - 1, -1) if back else range(num_features)
-    for it in its:
+    total = p if auto_feature else (p - num_features if back else num_features)
+    num_final = p if back else 0
+    for t in range(total):
+        it = p - 1 - t if back else t
         cands = [j for j in range(p) if mask[j] == (1 if back else 0)]
-        min_err, min_dim, min_k = FLT_MAX, -1, 0
+        min_err, min_dim, min_k, min_all = FLT_MAX, -1, 0, None
         for c in cands:
             d = (D - sq[:, :, c]) if back else (D + sq[:, :, c])
-            errs = []
             preds = np.zeros((len(kv), nr), np.float32)
             for r in range(nr):
                 ok = (~excl[r]) & (d[r] < FLT_MAX)
@@ -180,20 +255,31 @@ def np_select(prob, k_vals, num_features, method="forward"):
                 order = cols[np.lexsort((cols, d[r, cols]))][:kmax]
                 lst = np.zeros(kmax, np.int64)
                 lst[:order.size] = order
-                csum = np.add.accumulate(yc[lst], dtype=np.float32)
-                for m, k in enumerate(kv):
-                    preds[m, r] = np.float32(csum[k - 1] / np.float32(k))
-            best, bk = FLT_MAX, -1
-            for m, k in enumerate(kv):
-                e = yr - preds[m]
-                rm = rmse32(e * e)
-                if rm < best:
-                    best, bk = rm, int(k)
-            if bk >= 0 and best < min_err:
-                min_err, min_dim, min_k = best, c, bk
+                if model_type == 1:
+                    for m, k in enumerate(kv):
+                        preds[m, r] = np_mode(list(yc[lst[:k]]))
+                else:
+                    csum = np.add.accumulate(yc[lst], dtype=np.float32)
+                    for m, k in enumerate(kv):
+                        preds[m, r] = np.float32(csum[k - 1] / np.float32(k))
+            vals = np.array([[np_loss(yr, preds[m], lid) for m in range(len(kv))] for lid in lids], np.float32)
+            best, bm = FLT_MAX, -1
+            for m in range(len(kv)):
+                if vals[0, m] < best:
+                    best, bm = vals[0, m], m
+            if bm >= 0 and best < min_err:
+                min_err, min_dim, min_k, min_all = best, c, int(kv[bm]), vals[:, bm]
         mask[min_dim] = 0 if back else 1
         ordering[it] = min_dim
         errors[it] = min_err
+        errors_all[:, it] = min_all
         best_k_last = min_k
+        num_final = p - (t + 1) if back else t + 1
         D = (D - sq[:, :, min_dim]) if back else (D + sq[:, :, min_dim])
-    return {"ordering": ordering, "mask": mask, "errors": errors, "best_k": best_k_last}
+        if auto_feature:
+            if not back and it > 0 and errors[it - 1] < errors[it]:
+                break
+            if back and 0 < it < p - 1 and errors[it + 1] < errors[it]:
+                break
+    return {"ordering": ordering, "mask": mask, "errors": errors, "errors_all": errors_all, "best_k": best_k_last,
+            "num_final": num_final}

@@ -74,6 +74,8 @@ def lib():
             "snn_destroy": (ctypes.c_int, [vp]),
             "snn_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
             "snn_get_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]),
+            "snn_set_model": (ctypes.c_int, [vp, _i32p, ctypes.c_int, ctypes.c_int]),
+            "snn_get_errors_all": (ctypes.c_int, [vp, _f32p, ctypes.c_int]),
             "snn_batch_create": (ctypes.c_int, [ctypes.POINTER(SnnDesc), ctypes.c_int, ctypes.c_ulonglong,
                                                 ctypes.POINTER(vp)]),
             "snn_batch_load": (ctypes.c_int, [vp, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]),

@@ -71,13 +71,10 @@ class IncrementalNNFeatureSelection:
     def train(self):
         if self.method not in ("forward", "backward"):
             raise ValueError("Unknown feature selection method: %r" % (self.method,))
-        if self.model_type != 0:
-            raise NotImplementedError("classification models are not supported by speedynn_b200")
-        if list(self.loss_functions) != [0]:
-            raise NotImplementedError("speedynn_b200 scores candidates by RMSE only (loss_functions=['rmse'])")
         sel = Selector(self.Xtrain, self.Ytrain, self.Xval, self.Yval, k_vals=self.k_vals,
                        num_features=self.num_desired_features, method=self.method, k_fold=self.k_fold,
-                       auto_feature=bool(self.auto_feature), device=self.device)
+                       auto_feature=bool(self.auto_feature), device=self.device,
+                       loss_functions=self.loss_functions, model_type=self.model_type)
         try:
             r = sel.run()
         finally:
@@ -85,10 +82,8 @@ class IncrementalNNFeatureSelection:
         self.num_final_features = r["num_final"]
         self.selected_dimensions = r["mask"].astype(self.dtype_int)
         self.selected_ordering = r["ordering"].astype(self.dtype_int)
-        nl = self.loss_functions.shape[0]
-        errs = np.zeros((self.dim, nl), dtype=self.dtype_float)
-        errs[:, 0] = r["errors"]
-        self.selected_errors = errs
+        # speedynn/base.py:79-84 reshapes the flat [loss][p] array to (p, num_losses)
+        self.selected_errors = np.ascontiguousarray(r["errors_all"].T, dtype=self.dtype_float)
         self.selected_errors64 = r["errors64"]
         self.optimal_model_k = r["best_k"]
 

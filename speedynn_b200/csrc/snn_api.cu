@@ -81,6 +81,12 @@ struct snn_handle {
     int *kv = nullptr, *cands = nullptr, *prev_cands = nullptr, *mask = nullptr, *order = nullptr, *stepk = nullptr;
     int *perm = nullptr;           // candidate slot order: ascending training variance
     float *fvar = nullptr;         // per-feature training variance
+    // model: regression (kNN mean) or classification (mode), and the losses
+    int model = 0;
+    std::vector<int> loss_ids{0};  // reference loss ids; [0] decides
+    int *d_loss_ids = nullptr;
+    float *lossval = nullptr, *err_all = nullptr;
+    bool extra_losses() const { return !(loss_ids.size() == 1 && loss_ids[0] == 0); }
     State *st = nullptr;
     // pruned forward path
     float *Xrow = nullptr;        // training points, row-major
@@ -130,8 +136,13 @@ struct snn_handle {
         b.err64 = err64;
         b.stepk = stepk;
         b.st = st;
-        b.nn_idx = keep_nn ? nn_idx : nullptr;
-        b.nn_dist = keep_nn ? nn_dist : nullptr;
+        // classification predicts from the neighbour lists, so it always keeps them
+        b.nn_idx = keep_nn || model == 1 ? nn_idx : nullptr;
+        b.nn_dist = keep_nn || model == 1 ? nn_dist : nullptr;
+        b.nloss = extra_losses() ? (int)loss_ids.size() : 0;
+        b.loss_ids = d_loss_ids;
+        b.lossval = lossval;
+        b.err_all = err_all;
         return b;
     }
 };
@@ -158,7 +169,8 @@ void free_all(snn_handle *h)
     cudaSetDevice(h->device);
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar};
+                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar,
+                    h->d_loss_ids, h->lossval, h->err_all};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : h->score_ev) {
@@ -201,6 +213,7 @@ int check_device(int device)
 // commit, a k small enough for them, and shared memory for the lists.
 bool use_sparse(const snn_handle *h, int t, int n_cand)
 {
+    if (h->model == 1) return false;  // classification needs every list in full
     return h->prune && !h->desc.backward && t >= 1 && h->M > 0 && n_cand <= 128 &&
            snn::sparse_smem_per_warp(n_cand, h->kmax) <= (size_t)h->max_smem;
 }
@@ -232,7 +245,15 @@ int issue_step(snn_handle *h, int t)
     }
     SNN_CUDA(cudaEventRecord(se.b, h->stream));
     h->n_score++;
+    if (h->model == 1) {
+        SNN_CUDA(snn::launch_mode_predict(b, n_cand, h->stream));
+        h->n_launch += 1;
+    }
     SNN_CUDA(snn::launch_reduce(b, n_cand, h->stream));
+    if (b.nloss) {
+        SNN_CUDA(snn::launch_losses(b, n_cand, h->stream));
+        h->n_launch += 1;
+    }
     SNN_CUDA(snn::launch_select(b, n_cand, it, t, h->total_steps, backward, h->desc.auto_feature, h->stream));
     h->n_launch += 3;
     if (h->keep_nn) h->nn_ncand = n_cand;
@@ -563,6 +584,58 @@ SNN_API int snn_get_results(snn_handle *h, int *ordering, int *mask, float *erro
     if (int rc = read_state(h, &s)) return rc;
     if (best_k) *best_k = s.best_k_last;
     if (num_final) *num_final = s.num_final;
+    return SNN_OK;
+}
+
+SNN_API int snn_set_model(snn_handle *h, const int *loss_ids, int n_losses, int model_type)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!loss_ids || n_losses <= 0) return fail(SNN_ERR_ARG, "at least one loss id is required");
+    for (int l = 0; l < n_losses; ++l)
+        if (loss_ids[l] < 0 || loss_ids[l] > 8) return fail(SNN_ERR_ARG, "loss id %d is not one of 0..8", loss_ids[l]);
+    if (model_type != 0 && model_type != 1) return fail(SNN_ERR_ARG, "model_type %d is not 0 or 1", model_type);
+    SNN_CUDA(cudaSetDevice(h->device));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_loss_ids);
+    cudaFree(h->lossval);
+    cudaFree(h->err_all);
+    h->d_loss_ids = nullptr;
+    h->lossval = h->err_all = nullptr;
+    h->loss_ids.assign(loss_ids, loss_ids + n_losses);
+    h->model = model_type;
+    const size_t nl = (size_t)n_losses, p = (size_t)h->p;
+    if (h->extra_losses()) {
+        if (int rc = dev_alloc(&h->d_loss_ids, nl, "loss ids")) return rc;
+        if (int rc = dev_alloc(&h->lossval, nl * p * h->nk, "losses")) return rc;
+        if (int rc = dev_alloc(&h->err_all, nl * p, "losses per step")) return rc;
+        SNN_CUDA(cudaMemcpy(h->d_loss_ids, loss_ids, sizeof(int) * nl, cudaMemcpyHostToDevice));
+    }
+    if (model_type == 1 && !h->nn_idx) {
+        const size_t n = p * h->n_rows * h->kmax;
+        if (int rc = dev_alloc(&h->nn_idx, n, "neighbour indices")) return rc;
+        if (int rc = dev_alloc(&h->nn_dist, n, "neighbour distances")) return rc;
+    }
+    if (h->loaded) {
+        if (int rc = issue_reset(h)) return rc;
+        SNN_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    return SNN_OK;
+}
+
+SNN_API int snn_get_errors_all(snn_handle *h, float *errors, int n)
+{
+    g_err.clear();
+    if (!h || !errors) return fail(SNN_ERR_ARG, "null handle or output");
+    const size_t want = h->loss_ids.size() * (size_t)h->p;
+    if (n < (int)want) return fail(SNN_ERR_ARG, "errors needs %zu entries (losses x p)", want);
+    SNN_CUDA(cudaSetDevice(h->device));
+    if (h->extra_losses()) {
+        SNN_CUDA(cudaMemcpyAsync(errors, h->err_all, sizeof(float) * want, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        SNN_CUDA(cudaMemcpyAsync(errors, h->err, sizeof(float) * want, cudaMemcpyDeviceToHost, h->stream));
+    }
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
     return SNN_OK;
 }
 

@@ -6,9 +6,10 @@
 // results of the last run live in library state read by the get_* functions,
 // the return value is the final number of features.  Behaviour changed on
 // purpose: no exit()/printf on errors (negative status + snn_last_error()),
-// the n > 15000 "large scale" exit (nearest_neighbors_feature_selection.c:84-87)
-// does not exist, and every option outside kNN-regression RMSE selection is
-// rejected with SNN_ERR_UNSUPPORTED instead of running undefined code.
+// and the n > 15000 "large scale" exit (nearest_neighbors_feature_selection.c:84-87)
+// does not exist.  Loss lists and the classification model are passed to
+// snn_set_model; an unknown model type or loss id is rejected with
+// SNN_ERR_UNSUPPORTED instead of running undefined code.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -34,8 +35,13 @@ int train_common(int backward, float *X, int n, int d, float *y, int ny, int *kv
                  int *loss_functions, int nl, int auto_feature, int model_type)
 {
     if (!X || !y || !kvals || n <= 0 || d <= 0 || ny != n || nk <= 0) return SNN_ERR_ARG;
-    if (model_type != 0) return SNN_ERR_UNSUPPORTED;  // classification is not on this path
-    if (nl > 1 || (nl == 1 && (!loss_functions || loss_functions[0] != SNN_LOSS_RMSE))) return SNN_ERR_UNSUPPORTED;
+    if (model_type != 0 && model_type != 1) return SNN_ERR_UNSUPPORTED;
+    if (nl < 0 || (nl > 0 && !loss_functions)) return SNN_ERR_ARG;
+    static const int kRmseOnly[1] = {SNN_LOSS_RMSE};
+    const int *ids = nl > 0 ? loss_functions : kRmseOnly;
+    const int n_ids = nl > 0 ? nl : 1;
+    for (int l = 0; l < n_ids; ++l)
+        if (ids[l] < 0 || ids[l] > 8) return SNN_ERR_UNSUPPORTED;
     snn_desc desc;
     memset(&desc, 0, sizeof desc);
     desc.n_train = n;
@@ -52,15 +58,16 @@ int train_common(int backward, float *X, int n, int d, float *y, int ny, int *kv
     snn_handle *h = nullptr;
     int rc = snn_create(&desc, &h);
     if (rc) return rc;
-    rc = snn_load(h, X, y, nullptr, nullptr);
+    rc = snn_set_model(h, ids, n_ids, model_type);
+    if (!rc) rc = snn_load(h, X, y, nullptr, nullptr);
     if (!rc) rc = snn_run(h);
     LastRun r;
     r.mask.assign(d, 0);
     r.order.assign(d, 0);
-    r.errors.assign((size_t)std::max(nl, 1) * d, 0.0f);
+    r.errors.assign((size_t)n_ids * d, 0.0f);
     int num_final = 0;
-    if (!rc) rc = snn_get_results(h, r.order.data(), r.mask.data(), r.errors.data(), nullptr, nullptr, &r.best_k,
-                                  &num_final);
+    if (!rc) rc = snn_get_results(h, r.order.data(), r.mask.data(), nullptr, nullptr, nullptr, &r.best_k, &num_final);
+    if (!rc) rc = snn_get_errors_all(h, r.errors.data(), (int)r.errors.size());
     snn_destroy(h);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(g_mu);

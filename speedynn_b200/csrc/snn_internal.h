@@ -53,6 +53,11 @@ struct Bufs {
     State *st;
     int *nn_idx;      // optional [n_cand][n_rows][kmax]
     float *nn_dist;
+    // losses beyond the default RMSE (nloss 0: RMSE only, nothing recorded)
+    int nloss;
+    const int *loss_ids;  // [nloss] reference loss ids; index 0 decides
+    float *lossval;       // [nloss][n_cand][nk] this step's losses
+    float *err_all;       // [nloss][p] the winners' losses, reference order l * p + i
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D
@@ -102,6 +107,10 @@ cudaError_t launch_reduce(const Bufs &b, int n_cand, cudaStream_t s);
 cudaError_t launch_select(const Bufs &b, int n_cand, int it, int t, int total_steps, int backward,
                           int auto_feature, cudaStream_t s);
 cudaError_t launch_reset_state(const Bufs &b, int backward, int total_steps, cudaStream_t s);
+// Classification predictions from the kept neighbour lists (mode of the k labels).
+cudaError_t launch_mode_predict(const Bufs &b, int n_cand, cudaStream_t s);
+// Requested losses of every (candidate, k) prediction vector (b.nloss > 0).
+cudaError_t launch_losses(const Bufs &b, int n_cand, cudaStream_t s);
 // Per-feature training variance (FP64 sums) into var[p], NaN for non-finite columns.
 cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s);
 cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s);

@@ -197,7 +197,7 @@ __global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int
     if (st->done) return;
     float minv = FLT_MAX;
     double min64 = 0.0;
-    int wi = -1, wk = 0;
+    int wi = -1, wk = 0, wm = 0;
     for (int ci = 0; ci < n_cand; ++ci) {
         float best = FLT_MAX;
         int bm = -1;
@@ -213,6 +213,7 @@ __global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int
         if (best < minv || (best == minv && wi >= 0 && b.cands[ci] < b.cands[wi])) {
             minv = best;
             wi = ci;
+            wm = bm;
             wk = b.kvals[bm];
             min64 = b.rmse64[ci * b.nk + bm];
         }
@@ -229,6 +230,7 @@ __global__ void k_select(Bufs b, int n_cand, int it, int t, int total_steps, int
     b.err[it] = minv;
     b.err64[it] = min64;
     b.stepk[it] = wk;
+    for (int l = 0; l < b.nloss; ++l) b.err_all[l * b.p + it] = b.lossval[((size_t)l * n_cand + wi) * b.nk + wm];
     st->best_k_last = wk;
     b.mask[wdim] = backward ? 0 : 1;
     st->num_final = backward ? b.p - (t + 1) : t + 1;
@@ -283,6 +285,7 @@ __global__ void k_reset_state(Bufs b, int backward, int total_steps)
         b.stepk[j] = 0;
         b.cands[j] = b.perm[j];
         b.prev_cands[j] = b.perm[j];
+        for (int l = 0; l < b.nloss; ++l) b.err_all[l * b.p + j] = 0.0f;
     }
     if (j == 0) {
         State s;

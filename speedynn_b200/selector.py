@@ -25,7 +25,7 @@ class Selector:
     """
 
     def __init__(self, Xtrain, ytrain, Xval=None, yval=None, k_vals=(1, 2, 3, 4, 5, 6, 7, 8, 9), num_features=2,
-                 method="forward", k_fold=10, auto_feature=False, device=0):
+                 method="forward", k_fold=10, auto_feature=False, device=0, loss_functions=(0,), model_type=0):
         if method not in ("forward", "backward"):
             raise ValueError(f"unknown feature selection method {method!r}")
         L = _lib.lib()
@@ -58,7 +58,10 @@ class Selector:
         h = ctypes.c_void_p()
         check(L.snn_create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
+        self.loss_ids = np.ascontiguousarray(loss_functions, dtype=np.int32).reshape(-1)
         try:
+            if list(self.loss_ids) != [0] or int(model_type) != 0:
+                check(L.snn_set_model(h, ptr(self.loss_ids, _i32p), self.loss_ids.size, int(model_type)))
             check(L.snn_load(h, ptr(self.Xtrain, _f32p), ptr(self.ytrain, _f32p),
                              ptr(self.Xval, _f32p) if self.holdout else None,
                              ptr(self.yval, _f32p) if self.holdout else None))
@@ -94,6 +97,9 @@ class Selector:
                                          ptr(out["step_best_k"], _i32p), ctypes.byref(bk), ctypes.byref(nf)))
         out["best_k"] = bk.value
         out["num_final"] = nf.value
+        ea = np.zeros(self.loss_ids.size * p, np.float32)
+        check(_lib.lib().snn_get_errors_all(self._h, ptr(ea, _f32p), ea.size))
+        out["errors_all"] = ea.reshape(self.loss_ids.size, p)  # [loss][step slot], the reference's layout
         return out
 
     # -- inspection ------------------------------------------------------

@@ -5,13 +5,17 @@ sources (``oracle/_ref/libspeedynn_ref.so``) on seeded inputs and stores
 inputs + outputs as ``tests/golden/<case>.npz``.  Needs the reference sources
 (only this generator does); the committed .npz files are what the tests use.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                 # every fixture
+    python tests/golden/make_golden.py --only models   # the model_* cases (losses, classification)
 
 Each case stores: X, y, method, k_vals, num_features, k_fold, auto_feature and
 the reference outputs ordering, mask, errors (loss 0), best_k, num_final.
 Neighbour cases additionally store the lists returned by the reference's
 get_k_nearest_neighbors_cpu (speedynn/lib/cpu.c:212-252) after committing
-``committed`` with update_current_dist_matrix_cpu (cpu.c:301-315).
+``committed`` with update_current_dist_matrix_cpu (cpu.c:301-315).  Model
+cases (``model_*``) run the reference with a list of loss ids (the first
+decides) and the regression or classification model, and store every loss of
+every step (``errors_all``, the reference's [loss][p] layout).
 """
 import os
 import sys
@@ -86,6 +90,49 @@ def cases():
     return out
 
 
+def _classes(n, p, seed, n_cls=3):
+    """Integer class labels from a noisy linear rule on two features."""
+    X, _ = _gen(n, p, seed)
+    rng = np.random.default_rng(seed)
+    score = X[:, 0] - 0.7 * X[:, 2] + rng.normal(0, 0.4, n)
+    y = np.digitize(score, np.quantile(score, np.linspace(0, 1, n_cls + 1)[1:-1])).astype(np.float32)
+    return X, y
+
+
+def model_cases():
+    """(name, X, y, method, k_vals, num_features, k_fold, auto, loss ids, model type)."""
+    out = []
+    X, y = _gen(140, 9, 21)
+    out.append(("model_losses_fwd", X, y, "forward", [3, 7], 4, 5, False, [1, 0, 2, 3, 4, 5, 6, 7, 8], 0))
+    X, y = _gen(120, 10, 22)
+    out.append(("model_mad_bwd", X, y, "backward", [2, 5], 3, 4, False, [2, 0], 0))
+    X, y = _gen(90, 9, 23)
+    out.append(("model_std_fwd", X, y, "forward", [4], 3, 3, False, [5, 8, 0], 0))
+    X, y = _gen(110, 9, 27)
+    out.append(("model_rmse_norm_bwd_auto", X, y, "backward", [3], 2, 5, True, [1], 0))
+    X, y = _classes(150, 9, 24)
+    out.append(("model_classif_fwd", X, y, "forward", [1, 4, 6], 4, 5, False, [4, 0], 1))
+    X, y = _classes(130, 10, 25)
+    out.append(("model_classif_bwd", X, y, "backward", [3, 6], 2, 5, False, [4], 1))
+    X, y = _classes(160, 9, 26)
+    out.append(("model_classif_auto", X, y, "forward", [2, 5], 2, 4, True, [4, 2], 1))
+    return out
+
+
+def make_model_cases():
+    for name, X, y, method, kv, nf, kf, auto, losses, model in model_cases():
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        r = ref.train(X, y, kv, nf, kf, method, auto_feature=auto, loss_functions=losses, model_type=model)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), X=X, y=y, method=method,
+                            k_vals=np.asarray(kv, np.int32), num_features=nf, k_fold=kf, auto_feature=int(auto),
+                            loss_functions=np.asarray(losses, np.int32), model_type=model,
+                            ordering=r["ordering"], mask=r["mask"], errors_all=r["errors"], best_k=r["best_k"],
+                            num_final=r["num_final"])
+        print(f"{name}: n={X.shape[0]} p={X.shape[1]} {method} losses={losses} model={model} -> "
+              f"{r['ordering']} k*={r['best_k']}")
+
+
 NEIGHBOUR_CASES = [
     # (case, k_max, committed, method, candidates)
     ("extra_partial_fold", 5, [2], "forward", [0, 1, 3, 8]),
@@ -126,4 +173,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["--only", "models"]:
+        make_model_cases()
+    else:
+        main()
+        make_model_cases()

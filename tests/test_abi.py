@@ -95,16 +95,18 @@ def test_null_handle_calls_fail_cleanly(L):
 
 
 def test_dropin_rejects_unsupported_options(L):
+    """Loss ids outside the reference's 0..8 and model types other than
+    regression (0) / classification (1) are refused before any device work."""
     X = np.zeros((10, 3), np.float32)
     y = np.zeros(10, np.float32)
     kv = np.array([2], np.int32)
-    lf = np.array([2], np.int32)  # 'mad' as the deciding loss
+    lf = np.array([0, 9], np.int32)  # 9 is no reference loss
     rc = L.train_forward_selection(ptr(X, _f32p), 10, 3, ptr(y, _f32p), 10, ptr(kv, _i32p), 1, 2, 2, ptr(lf, _i32p),
-                                   1, 0, 0)
+                                   2, 0, 0)
     assert rc == _lib.SNN_ERR_UNSUPPORTED
-    lf[0] = 0
+    lf[1] = 2
     rc = L.train_forward_selection(ptr(X, _f32p), 10, 3, ptr(y, _f32p), 10, ptr(kv, _i32p), 1, 2, 2, ptr(lf, _i32p),
-                                   1, 0, 1)  # classification
+                                   2, 0, 2)  # model type 2 does not exist
     assert rc == _lib.SNN_ERR_UNSUPPORTED
 
 

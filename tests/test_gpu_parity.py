@@ -18,7 +18,7 @@ from speedynn_b200.selector import Selector
 pytestmark = pytest.mark.gpu
 
 GDIR = os.path.join(ROOT, "tests", "golden")
-SELECT_CASES = [n for n in golden_cases() if not n.startswith("nn_") and n != "losses"]
+SELECT_CASES = [n for n in golden_cases() if not n.startswith(("nn_", "model_")) and n != "losses"]
 NN_CASES = golden_cases("nn_")
 ERR64_RTOL = 1e-9
 

@@ -8,7 +8,7 @@ from conftest import ROOT, golden_cases
 from oracle import oracle, ref
 
 GDIR = os.path.join(ROOT, "tests", "golden")
-SELECT_CASES = [n for n in golden_cases() if not n.startswith("nn_") and n != "losses"]
+SELECT_CASES = [n for n in golden_cases() if not n.startswith(("nn_", "model_")) and n != "losses"]
 NN_CASES = golden_cases("nn_")
 
 
@@ -76,3 +76,22 @@ def test_live_reference_random_case():
         np.testing.assert_array_equal(o["ordering"], r["ordering"])
         np.testing.assert_array_equal(o["errors"], r["errors"][0])
         assert o["best_k"] == r["best_k"]
+
+
+MODEL_CASES = golden_cases("model_")
+
+
+@pytest.mark.parametrize("name", MODEL_CASES)
+def test_numpy_restatement_matches_reference_models(name):
+    """Loss lists (first decides) and the classification model: the NumPy
+    restatement reproduces speedynn's own outputs, every loss of every step."""
+    g = dict(np.load(os.path.join(GDIR, name + ".npz")))
+    prob = oracle.Problem(g["X"], g["y"], k_fold=int(g["k_fold"]))
+    o = oracle.np_select(prob, list(g["k_vals"]), int(g["num_features"]), str(g["method"]),
+                         loss_functions=list(g["loss_functions"]), model_type=int(g["model_type"]),
+                         auto_feature=bool(g["auto_feature"]))
+    np.testing.assert_array_equal(o["ordering"], g["ordering"])
+    np.testing.assert_array_equal(o["mask"], g["mask"])
+    np.testing.assert_array_equal(o["errors_all"], g["errors_all"])
+    assert o["best_k"] == int(g["best_k"])
+    assert o["num_final"] == int(g["num_final"])
