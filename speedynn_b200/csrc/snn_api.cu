@@ -86,6 +86,8 @@ struct snn_handle {
     std::vector<int> loss_ids{0};  // reference loss ids; [0] decides
     int *d_loss_ids = nullptr;
     float *lossval = nullptr, *err_all = nullptr;
+    float *kth_prev = nullptr;     // backward: last step's k-th distances [p][n_rows]
+    bool prev_ok = false;          // kth_prev holds the previous step's values
     bool extra_losses() const { return !(loss_ids.size() == 1 && loss_ids[0] == 0); }
     State *st = nullptr;
     // pruned forward path
@@ -143,6 +145,8 @@ struct snn_handle {
         b.loss_ids = d_loss_ids;
         b.lossval = lossval;
         b.err_all = err_all;
+        b.kth_prev = kth_prev;
+        b.use_prev = 0;
         return b;
     }
 };
@@ -170,7 +174,7 @@ void free_all(snn_handle *h)
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
                     h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar,
-                    h->d_loss_ids, h->lossval, h->err_all};
+                    h->d_loss_ids, h->lossval, h->err_all, h->kth_prev};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : h->score_ev) {
@@ -224,7 +228,7 @@ bool seeds_wanted(const snn_handle *h) { return h->prune && !h->desc.backward &&
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)
 {
-    const Bufs b = h->bufs();
+    Bufs b = h->bufs();
     const int n_cand = h->p - t;  // forward: p - t unselected; backward: p - t still selected
     const int backward = h->desc.backward;
     const int it = backward ? h->p - 1 - t : t;
@@ -232,18 +236,23 @@ int issue_step(snn_handle *h, int t)
     EventPair &se = h->score_ev[h->n_score];
     if (int rc = make_pair(se)) return rc;
     SNN_CUDA(cudaEventRecord(se.a, h->stream));
+    bool tma_step = false;
     if (use_sparse(h, t, n_cand)) {
         snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
         SNN_CUDA(snn::launch_score_sparse(b, sp, n_cand, h->M, h->max_smem, h->stream));
         h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
     } else if (h->kernel == 3 || (h->kernel == 0 && snn::score_tma_supported(h->kmax))) {
+        b.use_prev = backward && h->prev_ok ? 1 : 0;
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
+        h->prev_ok = backward && h->kth_prev;  // this step wrote every candidate's k-th distances
+        tma_step = true;
     } else if (h->kernel != 1 && snn::score_rw_supported(h->kmax)) {
         SNN_CUDA(snn::launch_score_rw(b, n_cand, backward, h->stream));
     } else {
         SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
     }
     SNN_CUDA(cudaEventRecord(se.b, h->stream));
+    if (!tma_step) h->prev_ok = false;
     h->n_score++;
     if (h->model == 1) {
         SNN_CUDA(snn::launch_mode_predict(b, n_cand, h->stream));
@@ -272,6 +281,7 @@ int issue_step(snn_handle *h, int t)
 
 int issue_reset(snn_handle *h)
 {
+    h->prev_ok = false;
     const Bufs b = h->bufs();
     SNN_CUDA(snn::launch_reset_state(b, h->desc.backward, h->total_steps, h->stream));
     if (h->desc.backward)
@@ -410,6 +420,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->cands, p, "candidates"))) return bail(rc);
     if ((rc = dev_alloc(&h->prev_cands, p, "candidates"))) return bail(rc);
     if ((rc = dev_alloc(&h->perm, p, "feature order"))) return bail(rc);
+    if (d->backward && (rc = dev_alloc(&h->kth_prev, p * (size_t)h->n_rows, "k-th distances"))) return bail(rc);
     if ((rc = dev_alloc(&h->fvar, p, "feature variances"))) return bail(rc);
     if ((rc = dev_alloc(&h->mask, p, "mask"))) return bail(rc);
     if ((rc = dev_alloc(&h->order, p, "ordering"))) return bail(rc);

@@ -58,6 +58,10 @@ struct Bufs {
     const int *loss_ids;  // [nloss] reference loss ids; index 0 decides
     float *lossval;       // [nloss][n_cand][nk] this step's losses
     float *err_all;       // [nloss][p] the winners' losses, reference order l * p + i
+    // backward: each (feature, row)'s k-th distance of the last step, [p][n_rows];
+    // removing a feature only lowers distances, so it bounds the next step's k-th
+    float *kth_prev;
+    int use_prev;         // 1: this step may take its bounds from kth_prev
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D

@@ -399,7 +399,10 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     __syncthreads();
 
     const int nstages = (b.ldc + kSC - 1) / kSC;
-    const int nA = nstages >= 4 ? nstages / 4 : 1;
+    // Backward steps after the first reuse the last step's k-th distances as
+    // bounds (D only shrinks when a feature is removed) and skip the first pass.
+    const bool reuse = BWD && b.use_prev && b.kth_prev != nullptr;
+    const int nA = reuse ? 0 : (nstages >= 4 ? nstages / 4 : 1);
     const int nvirt = nA + nstages;
 
     if (w == kConsumers) {
@@ -519,7 +522,14 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
             const float srt = warp_sort32(mn[p], lane);
             const float T = __shfl_sync(kFull, srt, (K - 1) & 31);
             float th;
-            if constexpr (BWD) th = T < FLT_MAX ? T : nextafterf(FLT_MAX, 0.0f);  // inclusive bound
+            if constexpr (BWD) {
+                float Tb = T;
+                if (reuse) {  // k distinct columns were at or below it last step and have not grown
+                    const int r = wr0 + p / kCW;
+                    Tb = (okmask >> p) & 1u ? b.kth_prev[(size_t)S.srcand[wc + p % kCW] * b.n_rows + r] : T;
+                }
+                th = Tb < FLT_MAX ? Tb : nextafterf(FLT_MAX, 0.0f);  // inclusive bound
+            }
             else th = (okmask >> p) & 1u ? fwd_bound(T) : -1.0f;                // padded: never passes
             if (lane == 0) myT[p] = th;
         }
@@ -661,8 +671,13 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     }
     if (!wvalid) return;
 
-    // Epilogue: optional neighbour dump, then labels gathered by all lanes and
-    // summed in rank order (sequential FP32, as the reference) by lane p.
+    // Epilogue: the k-th distances for the next backward step, the optional
+    // neighbour dump, then labels gathered by all lanes and summed in rank
+    // order (sequential FP32, as the reference) by lane p.
+    if (BWD && b.kth_prev && lane < kP && ((okmask >> lane) & 1u)) {
+        const int p = lane;
+        b.kth_prev[(size_t)S.srcand[wc + p % kCW] * b.n_rows + wr0 + p / kCW] = myL[p * KL + K - 1];
+    }
     if (b.nn_idx) {
         for (int p = 0; p < kP; ++p) {
             const int r = wr0 + p / kCW;
