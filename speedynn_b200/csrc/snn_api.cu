@@ -87,6 +87,7 @@ struct snn_handle {
     int *d_loss_ids = nullptr;
     float *lossval = nullptr, *err_all = nullptr;
     float *kth_prev = nullptr;     // backward: last step's k-th distances [p][n_rows]
+    float *dmax = nullptr;         // backward: per row, the largest finite entry of the full D
     bool prev_ok = false;          // kth_prev holds the previous step's values
     bool extra_losses() const { return !(loss_ids.size() == 1 && loss_ids[0] == 0); }
     State *st = nullptr;
@@ -147,6 +148,7 @@ struct snn_handle {
         b.err_all = err_all;
         b.kth_prev = kth_prev;
         b.use_prev = 0;
+        b.dmax = dmax;
         return b;
     }
 };
@@ -174,7 +176,7 @@ void free_all(snn_handle *h)
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
                     h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar,
-                    h->d_loss_ids, h->lossval, h->err_all, h->kth_prev};
+                    h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : h->score_ev) {
@@ -284,10 +286,13 @@ int issue_reset(snn_handle *h)
     h->prev_ok = false;
     const Bufs b = h->bufs();
     SNN_CUDA(snn::launch_reset_state(b, h->desc.backward, h->total_steps, h->stream));
-    if (h->desc.backward)
+    if (h->desc.backward) {
         SNN_CUDA(snn::launch_full_distance(b, h->cv, h->npf, h->stream));
-    else
+        SNN_CUDA(snn::launch_row_dmax(b, h->dmax, h->stream));
+        h->n_launch += 1;
+    } else {
         SNN_CUDA(snn::launch_init_forward(b, h->cv, h->npf, h->stream));
+    }
     h->n_launch += 2;
     h->host_step = 0;
     return SNN_OK;
@@ -421,6 +426,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->prev_cands, p, "candidates"))) return bail(rc);
     if ((rc = dev_alloc(&h->perm, p, "feature order"))) return bail(rc);
     if (d->backward && (rc = dev_alloc(&h->kth_prev, p * (size_t)h->n_rows, "k-th distances"))) return bail(rc);
+    if (d->backward && (rc = dev_alloc(&h->dmax, (size_t)h->n_rows, "row maxima"))) return bail(rc);
     if ((rc = dev_alloc(&h->fvar, p, "feature variances"))) return bail(rc);
     if ((rc = dev_alloc(&h->mask, p, "mask"))) return bail(rc);
     if ((rc = dev_alloc(&h->order, p, "ordering"))) return bail(rc);

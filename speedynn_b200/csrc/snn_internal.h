@@ -62,6 +62,7 @@ struct Bufs {
     // removing a feature only lowers distances, so it bounds the next step's k-th
     float *kth_prev;
     int use_prev;         // 1: this step may take its bounds from kth_prev
+    const float *dmax;    // backward: per row, >= every finite committed distance (filter margin)
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D
@@ -115,6 +116,8 @@ cudaError_t launch_reset_state(const Bufs &b, int backward, int total_steps, cud
 cudaError_t launch_mode_predict(const Bufs &b, int n_cand, cudaStream_t s);
 // Requested losses of every (candidate, k) prediction vector (b.nloss > 0).
 cudaError_t launch_losses(const Bufs &b, int n_cand, cudaStream_t s);
+// Per row of D: the largest finite entry (backward; D only shrinks afterwards).
+cudaError_t launch_row_dmax(const Bufs &b, float *dmax, cudaStream_t s);
 // Per-feature training variance (FP64 sums) into var[p], NaN for non-finite columns.
 cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s);
 cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s);

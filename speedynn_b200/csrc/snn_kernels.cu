@@ -301,6 +301,28 @@ __global__ void k_reset_state(Bufs b, int backward, int total_steps)
     }
 }
 
+// One block per row: the largest finite committed distance (non-negative
+// finite floats order like their bit patterns).  Backward elimination only
+// lowers D afterwards, so the value bounds the row for the whole run.
+__global__ void k_row_dmax(Bufs b, float *dmax)
+{
+    const int r = blockIdx.x;
+    const float *d = b.D + (size_t)r * b.ldc;
+    float m = 0.0f;
+    for (int i = threadIdx.x; i < b.n_cols; i += blockDim.x) {
+        const float v = d[i];
+        if (v < INFINITY && v > m) m = v;  // skips +inf (excluded pairs) and NaN
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
+        dmax[r] = fmaxf(m, red[0]);
+    }
+}
+
 // One block per feature: variance of the training column (FP64 sums).  Used
 // only to order candidate slots so that a scoring warp's candidates have
 // distances of similar scale; never part of a result.
@@ -394,6 +416,12 @@ cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, i
 cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s)
 {
     k_feature_variance<<<b.p, 256, 0, s>>>(b, var);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_row_dmax(const Bufs &b, float *dmax, cudaStream_t s)
+{
+    k_row_dmax<<<b.n_rows, 256, 0, s>>>(b, dmax);
     return cudaGetLastError();
 }
 

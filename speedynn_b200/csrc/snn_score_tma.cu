@@ -111,6 +111,17 @@ __device__ __forceinline__ float fwd_bound(float a)
 // u = fma(t, t, fl(D - H)) never misses a passing column.
 __device__ __forceinline__ float filter_bound(float T) { return fmaf(fmaxf(T, 0.0f), 1.0f + 0x1p-18f, 0x1p-125f); }
 
+// Backward filter bound: d = fl(D - fl(t*t)) <= T implies that the exact value
+// t*t + fl(H - D) is positive when H >= T+ (1 + 2^-19) + Dm 2^-21 + 2^-126,
+// Dm >= every finite D of the row (t*t <= D + T+ there, and fl(H - D) is off
+// by at most max(D, H) 2^-24).  A positive exact value keeps a clear sign bit
+// through the FMA's rounding, so u = fma(t, t, fl(H - D)) >= 0 (sign bit
+// clear) for every passing column.
+__device__ __forceinline__ float filter_bound_bwd(float T, float Dm)
+{
+    return fmaf(fmaxf(T, 0.0f), 1.0f + 0x1p-18f, fmaf(Dm, 0x1p-20f, 0x1p-125f));
+}
+
 __device__ __forceinline__ unsigned le_mask(float a, float b)
 {
     unsigned r;
@@ -187,78 +198,6 @@ __device__ __forceinline__ void tma_gather4(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
-// Insert (v, col) into the sorted list Ld/Li[0..K) with all 32 lanes; the
-// item goes after every element <= v.  Returns the new k-th distance.
-__device__ __forceinline__ float smem_list_insert(float *Ld, int *Li, int K, float v, int col, int lane)
-{
-    int pos = 0;
-    for (int g0 = 0; g0 < K; g0 += 32) {
-        const int x = g0 + lane;
-        const bool ok = x < K;
-        const float e = ok ? Ld[x] : INFINITY;
-        pos += __popc(__ballot_sync(kFull, ok && e <= v));
-    }
-    float carry = 0.0f;
-    int carryi = 0;
-    for (int g0 = 0; g0 < K; g0 += 32) {
-        const int x = g0 + lane;
-        const bool ok = x < K;
-        const float e = ok ? Ld[x] : INFINITY;
-        const int ix = ok ? Li[x] : 0;
-        float up = __shfl_up_sync(kFull, e, 1);
-        int upi = __shfl_up_sync(kFull, ix, 1);
-        if (lane == 0) {
-            up = carry;
-            upi = carryi;
-        }
-        carry = __shfl_sync(kFull, e, 31);
-        carryi = __shfl_sync(kFull, ix, 31);
-        if (ok && x >= pos) {
-            Ld[x] = (x == pos) ? v : up;
-            Li[x] = (x == pos) ? col : upi;
-        }
-    }
-    __syncwarp();
-    return Ld[K - 1];
-}
-
-// Rare path (out of line): insert the chunk's passing distances of the
-// warp's problems, problem by problem, lanes and columns in ascending order.
-template <bool BWD>
-__device__ __noinline__ void rare_path(unsigned pm, float *myL, int *myI, float *myT, const float *myX,
-                                       const float *D_w, const float *X_w, int q0, int colbase, int K, int KL)
-{
-    const int lane = threadIdx.x & 31;
-    unsigned wm = __reduce_or_sync(kFull, pm);
-    while (wm) {
-        const int p = __ffs(wm) - 1;
-        wm &= wm - 1;
-        unsigned m = __ballot_sync(kFull, (pm >> p) & 1u);
-        const float *drow = D_w + (p / kCW) * kSC + q0;
-        const float *xrow = X_w + (p % kCW) * kSC + q0;
-        const float xv = myX[p];
-        float th = myT[p];
-        float *L = myL + p * KL;
-        int *LI = myI + p * KL;
-        while (m) {
-            const int Lh = __ffs(m) - 1;
-            m &= m - 1;
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                const int c = 2 * Lh + h;
-                const float s1 = sqdiff1(xv, xrow[c]);
-                const float d = BWD ? __fsub_rn(drow[c], s1) : __fadd_rn(drow[c], s1);
-                if (d <= th) {
-                    const float kth = smem_list_insert(L, LI, K, d, colbase + c, lane);
-                    if (kth < FLT_MAX) th = nextafterf(kth, -INFINITY);
-                }
-            }
-        }
-        if (lane == 0) myT[p] = th;
-        __syncwarp();
-    }
-}
-
 // Largest float below x for 0 <= x < FLT_MAX (forward distances): turns the
 // strict test d < kth into the inclusive d <= below(kth).
 __device__ __forceinline__ float below(float x) { return x > 0.0f ? __int_as_float(__float_as_int(x) - 1) : -0x1p-149f; }
@@ -272,6 +211,7 @@ __device__ __forceinline__ float below(float x) { return x > 0.0f ? __int_as_flo
 // memory, and the list being filled sits in registers, lane j holding entry j.
 // Returns a mask of the warp's rows (bit p / kCW) whose thresholds may have
 // changed.
+template <bool BWD>
 __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, const float *X_s, const float *myX, float *myL,
                                           int *myI, float *myT, int q0, int colbase, int K, int KL)
 {
@@ -299,7 +239,8 @@ __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, 
             for (int h = 0; h < 2; ++h) {
                 if (!((hb >> h) & 1u)) continue;
                 const int c = 2 * l + h;
-                const float d = __fadd_rn(dr[c], sqdiff1(xv, xrow[c]));
+                const float s1 = sqdiff1(xv, xrow[c]);
+                const float d = BWD ? __fsub_rn(dr[c], s1) : __fadd_rn(dr[c], s1);
                 if (d <= th) {
                     // d < FLT_MAX and, for a full list, d < k-th: the slot is < K
                     const int pos = __popc(__ballot_sync(kFull, lane < K && Lj <= d));
@@ -313,7 +254,7 @@ __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, 
                         Ij = upI;
                     }
                     const float kth = __shfl_sync(kFull, Lj, K - 1);
-                    if (kth < FLT_MAX) th = below(kth);
+                    if (kth < FLT_MAX) th = BWD ? nextafterf(kth, -INFINITY) : below(kth);
                 }
             }
         }
@@ -456,7 +397,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     }
     // A padded problem (row past n_rows or candidate slot past n_cand) gets a
     // scored value that can never pass: NaN for backward (d = NaN), +inf for
-    // forward (d = D + inf = inf, and the forward filter value stays >= 0).
+    // forward (d = D + inf = inf, and the forward filter value stays >= 0);
+    // backward padded candidate slots on real rows are shadows (below).
     float2 xv2[kP];
     unsigned okmask = 0u;
 #pragma unroll
@@ -466,13 +408,22 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
             const int p = ri * kCW + ci;
             const int r = wr0 + ri;
             const bool okp = r < b.n_rows && c0 + wc + ci < n_cand;
-            const float x = okp ? __ldg(b.XV + (size_t)S.srcand[wc + ci] * b.ldr + r) : (BWD ? NAN : INFINITY);
+            // Backward scores a padded candidate slot as a shadow copy of a real
+            // candidate (srcand repeats cands[0]; nothing of it is written), so its
+            // filter flags no more often than a real problem's.
+            const bool live = BWD ? r < b.n_rows : okp;
+            const float x = live ? __ldg(b.XV + (size_t)S.srcand[wc + ci] * b.ldr + r) : (BWD ? NAN : INFINITY);
             xv2[p] = make_float2(x, x);
             okmask |= okp ? (1u << p) : 0u;
             if (lane == 0) myX[p] = x;
         }
     __syncwarp();
 
+    // backward: per-row bound on the finite committed distances (filter margin)
+    float myDm[kRW];
+#pragma unroll
+    for (int ri = 0; ri < kRW; ++ri)
+        myDm[ri] = !BWD || wr0 + ri >= b.n_rows ? 0.0f : b.dmax ? b.dmax[wr0 + ri] : FLT_MAX;  // no bound: flag all
     bool alive = true;
     // First pass over nA stages: per-lane minimum per problem.  Backward takes
     // the exact distance; forward takes a = fl(t*t + D) (one FMA), which is at
@@ -526,7 +477,7 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                 float Tb = T;
                 if (reuse) {  // k distinct columns were at or below it last step and have not grown
                     const int r = wr0 + p / kCW;
-                    Tb = (okmask >> p) & 1u ? b.kth_prev[(size_t)S.srcand[wc + p % kCW] * b.n_rows + r] : T;
+                    Tb = r < b.n_rows ? b.kth_prev[(size_t)S.srcand[wc + p % kCW] * b.n_rows + r] : T;
                 }
                 th = Tb < FLT_MAX ? Tb : nextafterf(FLT_MAX, 0.0f);  // inclusive bound
             }
@@ -536,22 +487,26 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
         __syncwarp();
     }
 
-    if constexpr (!BWD) {
-        // Forward full pass through a conservative filter.  Per scored row the
-        // warp keeps H = the largest filter_bound() of its four problems; a
+    {
+        // Full pass through a conservative filter.  Per scored row the warp
+        // keeps H = the largest filter bound of its four problems.  Forward: a
         // column can pass (d <= threshold) only if u = fl(t*t + fl(D - H)) < 0,
-        // so the hot loop costs one sub and one FMA per evaluation plus an OR
-        // of sign bits.  A row with a set sign bit is re-scored exactly.
+        // so the sign bits are ORed.  Backward (d = D - t*t): only if
+        // u = fl(t*t + fl(H - D)) >= 0, so the sign bits are ANDed and a clear
+        // bit flags the row.  The hot loop costs one sub and one FMA per
+        // evaluation; a flagged row is re-scored with the reference's rounding.
         float2 H2[kRW];
-        auto load_H = [&]() {
+        auto row_H = [&](int ri) {
+            float h = -INFINITY;
 #pragma unroll
-            for (int ri = 0; ri < kRW; ++ri) {
-                const float h = fmaxf(fmaxf(filter_bound(myT[ri * kCW + 0]), filter_bound(myT[ri * kCW + 1])),
-                                      fmaxf(filter_bound(myT[ri * kCW + 2]), filter_bound(myT[ri * kCW + 3])));
-                H2[ri] = make_float2(h, h);
+            for (int ci = 0; ci < kCW; ++ci) {
+                const float T = myT[ri * kCW + ci];
+                h = fmaxf(h, BWD ? filter_bound_bwd(T, myDm[ri]) : filter_bound(T));
             }
+            return make_float2(h, h);
         };
-        load_H();
+#pragma unroll
+        for (int ri = 0; ri < kRW; ++ri) H2[ri] = row_H(ri);
         for (int v = nA; v < nvirt && alive; ++v) {
             const int s = v % ring;
             if (!mbar_wait(S.full + s, (v / ring) & 1)) {
@@ -577,84 +532,43 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                     unsigned acc[kRW];
 #pragma unroll
                     for (int ri = 0; ri < kRW; ++ri) {
-                        const float2 E = sub2(dp[ri], H2[ri]);
+                        const float2 E = BWD ? sub2(H2[ri], dp[ri]) : sub2(dp[ri], H2[ri]);
                         float2 u[kCW];
 #pragma unroll
                         for (int ci = 0; ci < kCW; ++ci) {
                             const float2 t = sub2(xv2[ri * kCW + ci], xp[ci]);
                             u[ci] = fma2(t, t, E);
                         }
-                        acc[ri] = (f2u(u[0].x) | f2u(u[0].y) | f2u(u[1].x)) | (f2u(u[1].y) | f2u(u[2].x) | f2u(u[2].y)) |
-                                  (f2u(u[3].x) | f2u(u[3].y));
+                        if constexpr (BWD)
+                            acc[ri] = (f2u(u[0].x) & f2u(u[0].y) & f2u(u[1].x)) & (f2u(u[1].y) & f2u(u[2].x) & f2u(u[2].y)) &
+                                      (f2u(u[3].x) & f2u(u[3].y));
+                        else
+                            acc[ri] = (f2u(u[0].x) | f2u(u[0].y) | f2u(u[1].x)) | (f2u(u[1].y) | f2u(u[2].x) | f2u(u[2].y)) |
+                                      (f2u(u[3].x) | f2u(u[3].y));
                     }
-                    if (__any_sync(kFull, (int)((acc[0] | acc[1]) | (acc[2] | acc[3])) < 0)) {
+                    const unsigned all = BWD ? ((acc[0] & acc[1]) & (acc[2] & acc[3])) : ((acc[0] | acc[1]) | (acc[2] | acc[3]));
+                    if (__any_sync(kFull, BWD ? (int)all >= 0 : (int)all < 0)) {
                         unsigned pm = 0u;  // bit 2p+h: column 2*lane+h passes problem p exactly
 #pragma unroll
                         for (int ri = 0; ri < kRW; ++ri) {
-                            if (__any_sync(kFull, (int)acc[ri] < 0)) {
+                            if (__any_sync(kFull, BWD ? (int)acc[ri] >= 0 : (int)acc[ri] < 0)) {
 #pragma unroll
                                 for (int ci = 0; ci < kCW; ++ci) {
                                     const int p = ri * kCW + ci;
                                     const float th = myT[p];
-                                    const float2 e = add2(dp[ri], sq2(sub2(xv2[p], xp[ci])));
+                                    const float2 s2 = sq2(sub2(xv2[p], xp[ci]));
+                                    const float2 e = BWD ? sub2(dp[ri], s2) : add2(dp[ri], s2);
                                     pm |= (le_mask(e.x, th) & (1u << (2 * p))) | (le_mask(e.y, th) & (2u << (2 * p)));
                                 }
                             }
                         }
                         if (__any_sync(kFull, pm != 0u)) {
-                            const unsigned rows = insert_chunk(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K, KL);
+                            const unsigned rows =
+                                insert_chunk<BWD>(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K, KL);
 #pragma unroll
                             for (int ri = 0; ri < kRW; ++ri)
-                                if ((rows >> ri) & 1u) {
-                                    const float h = fmaxf(fmaxf(filter_bound(myT[ri * kCW + 0]), filter_bound(myT[ri * kCW + 1])),
-                                                          fmaxf(filter_bound(myT[ri * kCW + 2]), filter_bound(myT[ri * kCW + 3])));
-                                    H2[ri] = make_float2(h, h);
-                                }
+                                if ((rows >> ri) & 1u) H2[ri] = row_H(ri);
                         }
-                    }
-                }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(S.empty + s);
-        }
-    } else {
-        // Backward full pass: exact distances, threshold compare per element.
-        float thr[kP];
-#pragma unroll
-        for (int p = 0; p < kP; ++p) thr[p] = myT[p];
-        for (int v = nA; v < nvirt && alive; ++v) {
-            const int s = v % ring;
-            if (!mbar_wait(S.full + s, (v / ring) & 1)) {
-                alive = false;
-                break;
-            }
-            const int i0 = (v - nA) * kSC;
-            const int cols = min(kSC, b.ldc - i0);
-            const float *D_w = S.Ds + (s * kRowsB + rg * kRW) * kSC;
-            const float *X_w = S.Xs + (s * kCandB + wc) * kSC;
-            if (wvalid) {
-#pragma unroll 2
-                for (int q0 = 0; q0 < cols; q0 += kChunk) {
-                    float2 dp[kRW], xp[kCW];
-#pragma unroll
-                    for (int ri = 0; ri < kRW; ++ri)
-                        dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0 + 2 * lane);
-#pragma unroll
-                    for (int ci = 0; ci < kCW; ++ci)
-                        xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0 + 2 * lane);
-                    unsigned pm = 0u;
-#pragma unroll
-                    for (int ri = 0; ri < kRW; ++ri)
-#pragma unroll
-                        for (int ci = 0; ci < kCW; ++ci) {
-                            const int p = ri * kCW + ci;
-                            const float2 e = sub2(dp[ri], sq2(sub2(xv2[p], xp[ci])));
-                            pm |= (le_mask(e.x, thr[p]) | le_mask(e.y, thr[p])) & (1u << p);
-                        }
-                    if (__any_sync(kFull, pm != 0u)) {
-                        rare_path<true>(pm, myL, myI, myT, myX, D_w, X_w, q0, i0 + q0, K, KL);
-#pragma unroll
-                        for (int p = 0; p < kP; ++p) thr[p] = myT[p];
                     }
                 }
             }

@@ -252,3 +252,45 @@ def test_large_problem_sampled_rows_match_oracle(kv):
     o = oracle.step(prob, kv, committed, list(cands), rows=rows)
     np.testing.assert_array_equal(idx[:, rows], o["nn_idx"])
     np.testing.assert_array_equal(dist[:, rows], o["nn_dist"])
+
+
+def test_noalloc_backward_step_matches_handle():
+    """The allocation-free entry point on a backward step (it has no per-row
+    distance maxima, so its backward filter flags every chunk and scores it
+    exactly): same winner, best k and FP32 error as a handle's first step."""
+    import ctypes
+
+    import torch
+
+    s = datagen.generate(1500, 400, 11, n_mag=5, seed=73)
+    k_vals = np.array([4, 9], np.int32)
+    n_tr, n_val, p = s.Xtrain.shape[0], s.Xval.shape[0], s.Xtrain.shape[1]
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=k_vals, num_features=p - 1, method="backward") as sel:
+        ref = sel.run()
+    want = (int(ref["ordering"][p - 1]), int(ref["step_best_k"][p - 1]), ref["errors"][p - 1])
+    ld = (n_tr + 63) // 64 * 64
+    Dh = np.zeros((n_val, ld), np.float32)
+    for k in range(p - 1, -1, -1):  # full distance, dims in descending order
+        diff = s.Xval[:, k][:, None] - s.Xtrain[:, k][None, :]
+        Dh[:, :n_tr] = Dh[:, :n_tr] + diff * diff
+    Dh[:, n_tr:] = np.inf
+    dev = torch.device("cuda", 0)
+    D = torch.from_numpy(Dh).to(dev)
+    XT = torch.zeros((p, ld), dtype=torch.float32, device=dev)
+    XT[:, :n_tr] = torch.from_numpy(np.ascontiguousarray(s.Xtrain.T)).to(dev)
+    XV = torch.from_numpy(np.ascontiguousarray(s.Xval.T)).to(dev)
+    yt = torch.from_numpy(s.ytrain).to(dev)
+    yv = torch.from_numpy(s.yval).to(dev)
+    cands = np.arange(p, dtype=np.int32)
+    e32 = torch.zeros((p, k_vals.size), dtype=torch.float32, device=dev)
+    e64 = torch.zeros((p, k_vals.size), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    L = _lib.lib()
+    rc = L.snn_score_step_noalloc(D.data_ptr(), ld, XT.data_ptr(), XV.data_ptr(), n_val, yt.data_ptr(), yv.data_ptr(),
+                                  n_val, n_tr, p, ptr(cands, _i32p), p, ptr(k_vals, _i32p), k_vals.size, 1,
+                                  e32.data_ptr(), e64.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    assert rc == 0, _lib.last_error()
+    err = e32.cpu().numpy()
+    best = [(err[c].min(), c, int(k_vals[int(np.argmin(err[c]))])) for c in range(p)]
+    e, c, k = min(best, key=lambda t: (t[0], t[1]))
+    assert (c, k) == want[:2] and e == want[2]
