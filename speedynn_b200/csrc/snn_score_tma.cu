@@ -16,12 +16,13 @@
 //     stalling the others.
 //   * First pass over a quarter of the columns: per-lane minima; their k-th
 //     smallest bounds the final k-th distance (k distinct columns lie at or
-//     below it).
-//   * Full pass, forward: a conservative sign-bit filter (one sub and one FMA
-//     per evaluation, see filter_bound) flags rows that may hold a passing
-//     column; flagged rows are re-scored with the reference's rounding and
-//     passes are inserted in column order (d <= T until the list is full,
-//     then d < k-th).  Backward: exact distances and a compare per element.
+//     below it).  Backward steps after the first skip it and start from the
+//     previous step's k-th distances (kth_prev), which removal only lowers.
+//   * Full pass: a conservative sign-bit filter (one sub and one FMA per
+//     evaluation; filter_bound / filter_bound_bwd) flags rows that may hold a
+//     passing column; flagged rows are re-scored with the reference's
+//     rounding and passes are inserted in column order (d <= T until the list
+//     is full, then d < k-th).
 //   * Every wait is bounded: on timeout the warp records SNN_ERR_TIMEOUT in
 //     the device state and leaves (the producer first drains its copies).
 #include <cuda.h>
