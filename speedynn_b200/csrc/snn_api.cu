@@ -89,6 +89,8 @@ struct snn_handle {
     float *kth_prev = nullptr;     // backward: last step's k-th distances [p][n_rows]
     float *dmax = nullptr;         // backward: per row, the largest finite entry of the full D
     bool prev_ok = false;          // kth_prev holds the previous step's values
+    int inject_stall = -1;         // fault injection (see dev_alloc): stage to withhold once
+    int inject_launch = -1;        // fault injection: greedy step whose launch fails once
     bool extra_losses() const { return !(loss_ids.size() == 1 && loss_ids[0] == 0); }
     State *st = nullptr;
     // pruned forward path
@@ -149,16 +151,25 @@ struct snn_handle {
         b.kth_prev = kth_prev;
         b.use_prev = 0;
         b.dmax = dmax;
+        b.inject_stall = 0;
         return b;
     }
 };
 
 namespace {
 
+// Fault injection for tests (environment, read by snn_create; each fires once):
+//   SNN_INJECT_FAIL=alloc:N   the N-th device allocation of that snn_create fails (SNN_ERR_NOMEM)
+//   SNN_INJECT_FAIL=launch:N  the scoring launch of greedy step N fails (SNN_ERR_CUDA)
+//   SNN_INJECT_STALL=N        block 0 of the next TMA-fed scoring launch never issues the copies
+//                             of stage N, so its bounded waits run out (SNN_ERR_TIMEOUT)
+thread_local int t_fail_alloc = 0;  // countdown to the injected allocation failure, 0 = off
+
 template <typename T>
 int dev_alloc(T **p, size_t n, const char *what)
 {
     *p = nullptr;
+    if (t_fail_alloc > 0 && --t_fail_alloc == 0) return fail(SNN_ERR_NOMEM, "injected failure of the allocation of %s", what);
     if (n == 0) n = 1;
     cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
     if (e != cudaSuccess) {
@@ -238,6 +249,10 @@ int issue_step(snn_handle *h, int t)
     EventPair &se = h->score_ev[h->n_score];
     if (int rc = make_pair(se)) return rc;
     SNN_CUDA(cudaEventRecord(se.a, h->stream));
+    if (t == h->inject_launch) {
+        h->inject_launch = -1;
+        return fail(SNN_ERR_CUDA, "injected launch failure at step %d", t);
+    }
     bool tma_step = false;
     if (use_sparse(h, t, n_cand)) {
         snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
@@ -245,6 +260,8 @@ int issue_step(snn_handle *h, int t)
         h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
     } else if (h->kernel == 3 || (h->kernel == 0 && snn::score_tma_supported(h->kmax))) {
         b.use_prev = backward && h->prev_ok ? 1 : 0;
+        b.inject_stall = h->inject_stall + 1;  // 0: off
+        h->inject_stall = -1;
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
         h->prev_ok = backward && h->kth_prev;  // this step wrote every candidate's k-th distances
         tma_step = true;
@@ -371,6 +388,11 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (int rc = check_device(d->device)) return rc;
 
     snn_handle *h = new snn_handle();
+    if (const char *f = getenv("SNN_INJECT_FAIL")) {
+        if (!strncmp(f, "alloc:", 6)) t_fail_alloc = atoi(f + 6);
+        if (!strncmp(f, "launch:", 7)) h->inject_launch = atoi(f + 7);
+    }
+    if (const char *f = getenv("SNN_INJECT_STALL")) h->inject_stall = atoi(f);
     h->desc = *d;
     h->kvals.assign(d->k_vals, d->k_vals + d->num_k_vals);
     h->desc.k_vals = nullptr;
@@ -391,6 +413,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
 
     int rc = SNN_OK;
     auto bail = [&](int code) {
+        t_fail_alloc = 0;
         free_all(h);
         delete h;
         return code;
@@ -439,6 +462,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (cudaMemcpy(h->kv, h->kvals.data(), sizeof(int) * h->nk, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(SNN_ERR_CUDA, "copy of k_vals failed"));
     if (make_pair(h->total_ev)) return bail(SNN_ERR_CUDA);
+    t_fail_alloc = 0;
     *out = h;
     return SNN_OK;
 }

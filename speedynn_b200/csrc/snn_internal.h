@@ -63,6 +63,7 @@ struct Bufs {
     float *kth_prev;
     int use_prev;         // 1: this step may take its bounds from kth_prev
     const float *dmax;    // backward: per row, >= every finite committed distance (filter margin)
+    int inject_stall;     // test hook, 0 off: block 0 never issues the copies of stage inject_stall - 1
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D

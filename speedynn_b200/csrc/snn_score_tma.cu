@@ -364,6 +364,10 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                     break;
                 }
                 const int i0 = (v < nA ? v : v - nA) * kSC;
+                if (blockIdx.x == 0 && v + 1 == b.inject_stall) {  // test hook: the consumers' waits run out
+                    issued = v + 1;
+                    continue;
+                }
                 mbar_arrive_expect_tx(S.full + s, kStageBytes);
                 tma_tile_2d(S.Ds + s * kRowsB * kSC, &tmD, i0, r0, S.full + s);
 #pragma unroll
