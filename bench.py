@@ -349,6 +349,11 @@ def run_ours(args, world, rank, local):
     wall = time.perf_counter() - t0
     clocks = clk.stop()
     res = sel.results()
+    # one more selection with the filter counters on (outside the timed region)
+    sel.set_counters(True)
+    sel.run()
+    fc = sel.filter_counters()
+    sel.set_counters(False)
     ms_step = allmax(tot_ms / args.steps, world)
 
     # end to end through the public API: pinned host inputs uploaded every step, results read back
@@ -400,6 +405,12 @@ def run_ours(args, world, rank, local):
             "e2e": None if args.no_e2e else {"value": world * evals / e2e_s, "unit": UNIT,
                                              "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
+            "filter": {"row_chunks": fc["row_chunks"],
+                       "flagged_frac": fc["flagged"] / fc["row_chunks"] if fc["row_chunks"] else None,
+                       "passing_frac": fc["passed"] / fc["row_chunks"] if fc["row_chunks"] else None,
+                       "note": "(row, 64-column chunk) pairs of the TMA-fed scorer's full passes in one selection "
+                               "(counted in an extra untimed run); flagged = re-scored exactly, passing = held a "
+                               "list update candidate"},
             "roofline": {"bound": "fp32", "kernel": scoring_kernel(k, args.kernel), "achieved": achieved_fp32,
                          "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved_fp32 / fp32_peak,

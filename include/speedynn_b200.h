@@ -194,11 +194,27 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
  *                  Results are identical; this exists for cross-checks and
  *                  measurement. */
 #define SNN_OPT_KERNEL 2
+/*   SNN_OPT_COUNTERS 1: the TMA-fed scorer keeps the filter counters read by
+ *                  snn_get_filter_counters (a little slower).  Default 0. */
+#define SNN_OPT_COUNTERS 3
 SNN_API int snn_set_option(snn_handle *h, int option, int value);
 
 /* Work counters since the last run/step/reset: (row, column) pairs the pruned
  * scorer streamed, and how many of them it had to score. */
 SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, unsigned long long *pairs_survived);
+
+/* Tracing of the TMA-fed scorer since the last run/step/reset: (row, chunk)
+ * pairs of its full passes (a chunk = 64 training columns), how many the
+ * sign-bit filter flagged for exact re-scoring, and how many of those held a
+ * passing column.  Kept by that scorer only (k_max <= 32) and only while
+ * SNN_OPT_COUNTERS is set. */
+SNN_API int snn_get_filter_counters(snn_handle *h, unsigned long long *row_chunks, unsigned long long *flagged,
+                                    unsigned long long *passed);
+
+/* CUDA-event milliseconds of each greedy step of the last run/step calls:
+ * score_ms[i] and commit_ms[i] for i < n (0 past the steps run).  Returns the
+ * number of steps timed. */
+SNN_API int snn_get_step_timing(snn_handle *h, float *score_ms, float *commit_ms, int n);
 
 SNN_API int snn_destroy(snn_handle *h);
 

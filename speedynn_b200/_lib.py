@@ -22,6 +22,7 @@ SNN_ERR_TIMEOUT = -7
 
 SNN_OPT_PRUNE = 1
 SNN_OPT_KERNEL = 2
+SNN_OPT_COUNTERS = 3
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -76,6 +77,10 @@ def lib():
             "snn_get_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]),
             "snn_set_model": (ctypes.c_int, [vp, _i32p, ctypes.c_int, ctypes.c_int]),
             "snn_get_errors_all": (ctypes.c_int, [vp, _f32p, ctypes.c_int]),
+            "snn_get_filter_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong),
+                                                       ctypes.POINTER(ctypes.c_ulonglong),
+                                                       ctypes.POINTER(ctypes.c_ulonglong)]),
+            "snn_get_step_timing": (ctypes.c_int, [vp, _f32p, _f32p, ctypes.c_int]),
             "snn_batch_create": (ctypes.c_int, [ctypes.POINTER(SnnDesc), ctypes.c_int, ctypes.c_ulonglong,
                                                 ctypes.POINTER(vp)]),
             "snn_batch_load": (ctypes.c_int, [vp, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]),

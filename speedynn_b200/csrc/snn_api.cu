@@ -98,6 +98,8 @@ struct snn_handle {
     int *seeds = nullptr;         // [n_rows][M]
     int M = 0;
     unsigned long long *survivors = nullptr;
+    unsigned long long *fcount = nullptr;  // filter counters of the TMA-fed scorer (3)
+    bool count_filter = false;             // SNN_OPT_COUNTERS
     bool prune = false;           // measured slower than the full scan on dense data; opt in
     int kernel = 0;               // scoring kernel: 0 auto, 1 rows-per-lane, 2 row-per-warp
     int max_smem = 0;
@@ -152,6 +154,7 @@ struct snn_handle {
         b.use_prev = 0;
         b.dmax = dmax;
         b.inject_stall = 0;
+        b.fcount = count_filter ? fcount : nullptr;
         return b;
     }
 };
@@ -187,7 +190,7 @@ void free_all(snn_handle *h)
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
                     h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar,
-                    h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax};
+                    h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : h->score_ev) {
@@ -327,6 +330,7 @@ void reset_timing(snn_handle *h)
     h->n_score = h->n_commit = h->n_launch = 0;
     h->scanned_pairs = 0;
     if (h->survivors) cudaMemsetAsync(h->survivors, 0, sizeof(unsigned long long), h->stream);
+    if (h->fcount) cudaMemsetAsync(h->fcount, 0, 3 * sizeof(unsigned long long), h->stream);
 }
 
 }  // namespace
@@ -457,6 +461,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->st, 1, "state"))) return bail(rc);
     if ((rc = dev_alloc(&h->Xrow, p * h->n_cols, "X_train rows"))) return bail(rc);
     if ((rc = dev_alloc(&h->survivors, 1, "counters"))) return bail(rc);
+    if ((rc = dev_alloc(&h->fcount, 3, "filter counters"))) return bail(rc);
     h->M = d->backward ? 0 : snn::seeds_for_k(kmax);
     if (h->M > 0 && (rc = dev_alloc(&h->seeds, (size_t)h->n_rows * h->M, "seed columns"))) return bail(rc);
     if (cudaMemcpy(h->kv, h->kvals.data(), sizeof(int) * h->nk, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -760,6 +765,7 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value)
             return fail(SNN_ERR_UNSUPPORTED, "the TMA-fed kernel handles k_max <= 32");
         h->kernel = value;
         return SNN_OK;
+    case SNN_OPT_COUNTERS: h->count_filter = value != 0; return SNN_OK;
     default: return fail(SNN_ERR_ARG, "unknown option %d", option);
     }
 }
@@ -775,6 +781,42 @@ SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, 
     if (pairs_streamed) *pairs_streamed = h->scanned_pairs;
     if (pairs_survived) *pairs_survived = sv;
     return SNN_OK;
+}
+
+SNN_API int snn_get_filter_counters(snn_handle *h, unsigned long long *row_chunks, unsigned long long *flagged,
+                                    unsigned long long *passed)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    SNN_CUDA(cudaSetDevice(h->device));
+    unsigned long long c[3] = {0, 0, 0};
+    SNN_CUDA(cudaMemcpyAsync(c, h->fcount, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    if (row_chunks) *row_chunks = c[0];
+    if (flagged) *flagged = c[1];
+    if (passed) *passed = c[2];
+    return SNN_OK;
+}
+
+SNN_API int snn_get_step_timing(snn_handle *h, float *score_ms, float *commit_ms, int n)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    SNN_CUDA(cudaSetDevice(h->device));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < n; ++i) {
+        float ms = 0.f;
+        if (score_ms) {
+            if (i < h->n_score) SNN_CUDA(cudaEventElapsedTime(&ms, h->score_ev[i].a, h->score_ev[i].b));
+            score_ms[i] = i < h->n_score ? ms : 0.f;
+        }
+        if (commit_ms) {
+            ms = 0.f;
+            if (i < h->n_commit) SNN_CUDA(cudaEventElapsedTime(&ms, h->commit_ev[i].a, h->commit_ev[i].b));
+            commit_ms[i] = i < h->n_commit ? ms : 0.f;
+        }
+    }
+    return h->n_score;
 }
 
 SNN_API int snn_destroy(snn_handle *h)

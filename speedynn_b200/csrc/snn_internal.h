@@ -64,6 +64,9 @@ struct Bufs {
     int use_prev;         // 1: this step may take its bounds from kth_prev
     const float *dmax;    // backward: per row, >= every finite committed distance (filter margin)
     int inject_stall;     // test hook, 0 off: block 0 never issues the copies of stage inject_stall - 1
+    // optional filter counters of the TMA-fed scorer: [0] (row, chunk) pairs of
+    // the full pass, [1] of them flagged by the filter, [2] holding an exact pass
+    unsigned long long *fcount;
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D

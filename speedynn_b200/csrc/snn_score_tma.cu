@@ -289,7 +289,7 @@ __device__ __forceinline__ float warp_sort32(float v, int lane)
 
 struct TmaSmem {
     float *Ds, *Xs, *Lds, *thr_s, *xv_s;
-    int *Lis, *srcand;
+    int *Lis, *srcand, *wcnt;
     uint64_t *full, *empty;
     int *flag;
 };
@@ -309,10 +309,11 @@ __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL, int ri
     S.xv_s = S.thr_s + kConsumers * kP;
     S.srcand = reinterpret_cast<int *>(S.xv_s + kConsumers * kP);      // [kCandB]
     S.flag = S.srcand + kCandB;
+    S.wcnt = S.flag + 1;  // [kConsumers][2] flagged / passing (row, chunk) pairs
     return S;
 }
 
-template <bool BWD, int ring>
+template <bool BWD, int ring, bool COUNT>
 __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg, const __grid_constant__ CUtensorMap tmD,
                                                                    const __grid_constant__ CUtensorMap tmX)
 {
@@ -396,6 +397,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     int *myI = S.Lis + w * kP * KL;
     float *myT = S.thr_s + w * kP;
     float *myX = S.xv_s + w * kP;
+    int *myCnt = S.wcnt + 2 * w;
+    if (COUNT && lane == 0) myCnt[0] = myCnt[1] = 0;
     for (int e = lane; e < kP * KL; e += 32) {
         myL[e] = (e % KL) < K ? FLT_MAX : INFINITY;
         myI[e] = 0;
@@ -554,9 +557,11 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                     const unsigned all = BWD ? ((acc[0] & acc[1]) & (acc[2] & acc[3])) : ((acc[0] | acc[1]) | (acc[2] | acc[3]));
                     if (__any_sync(kFull, BWD ? (int)all >= 0 : (int)all < 0)) {
                         unsigned pm = 0u;  // bit 2p+h: column 2*lane+h passes problem p exactly
+                        int nfl = 0;
 #pragma unroll
                         for (int ri = 0; ri < kRW; ++ri) {
                             if (__any_sync(kFull, BWD ? (int)acc[ri] >= 0 : (int)acc[ri] < 0)) {
+                                if constexpr (COUNT) ++nfl;
 #pragma unroll
                                 for (int ci = 0; ci < kCW; ++ci) {
                                     const int p = ri * kCW + ci;
@@ -565,6 +570,16 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                                     const float2 e = BWD ? sub2(dp[ri], s2) : add2(dp[ri], s2);
                                     pm |= (le_mask(e.x, th) & (1u << (2 * p))) | (le_mask(e.y, th) & (2u << (2 * p)));
                                 }
+                            }
+                        }
+                        if constexpr (COUNT) {
+                            const unsigned pmw = __reduce_or_sync(kFull, pm);
+                            if (lane == 0) {
+                                unsigned rp = 0u;  // rows holding a pass
+#pragma unroll
+                                for (int ri = 0; ri < kRW; ++ri) rp |= ((pmw >> (8 * ri)) & 0xffu) ? (1u << ri) : 0u;
+                                myCnt[0] += nfl;
+                                myCnt[1] += __popc(rp);
                             }
                         }
                         if (__any_sync(kFull, pm != 0u)) {
@@ -580,6 +595,11 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
             __syncwarp();
             if (lane == 0) mbar_arrive(S.empty + s);
         }
+    }
+    if (COUNT && wvalid && lane == 0) {
+        atomicAdd(b.fcount + 0, (unsigned long long)kRW * (unsigned long long)(b.ldc / kChunk));
+        atomicAdd(b.fcount + 1, (unsigned long long)myCnt[0]);
+        atomicAdd(b.fcount + 2, (unsigned long long)myCnt[1]);
     }
     if (!alive) {
         if (lane == 0) {
@@ -636,7 +656,7 @@ size_t tma_smem_bytes(int K, int ring)
     const int KL = list_slots(K);
     return kBarBytes + sizeof(float) * (size_t)ring * (kRowsB + kCandB) * kSC +
            (sizeof(float) + sizeof(int)) * (size_t)kConsumers * kP * KL + 2 * sizeof(float) * kConsumers * kP +
-           sizeof(int) * (kCandB + 1);
+           sizeof(int) * (kCandB + 1 + 2 * kConsumers);
 }
 
 }  // namespace
@@ -693,8 +713,12 @@ cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream
     const bool deep = list_slots(b.kmax) == 16;
     const size_t smem = tma_smem_bytes(b.kmax, deep ? kRingDeep : kRingShallow);
     if (smem > (size_t)max_smem) return cudaErrorInvalidConfiguration;
-    auto kern = backward ? (deep ? k_score_tma<true, kRingDeep> : k_score_tma<true, kRingShallow>)
-                         : (deep ? k_score_tma<false, kRingDeep> : k_score_tma<false, kRingShallow>);
+    // the counting variants are separate instantiations: the default code has no counting at all
+    const bool cnt = b.fcount != nullptr;
+    auto kern = backward ? (deep ? (cnt ? k_score_tma<true, kRingDeep, true> : k_score_tma<true, kRingDeep, false>)
+                                 : (cnt ? k_score_tma<true, kRingShallow, true> : k_score_tma<true, kRingShallow, false>))
+                         : (deep ? (cnt ? k_score_tma<false, kRingDeep, true> : k_score_tma<false, kRingDeep, false>)
+                                 : (cnt ? k_score_tma<false, kRingShallow, true> : k_score_tma<false, kRingShallow, false>));
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)blocks, (kConsumers + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);

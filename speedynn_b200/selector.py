@@ -133,6 +133,24 @@ class Selector:
         check(_lib.lib().snn_get_counters(self._h, ctypes.byref(a), ctypes.byref(b)))
         return {"pairs_streamed": a.value, "pairs_survived": b.value}
 
+    def set_counters(self, enable):
+        """Keep the TMA-fed scorer's filter counters (off by default: a little slower)."""
+        check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_COUNTERS, int(bool(enable))))
+
+    def filter_counters(self):
+        """(row, chunk) pairs of the TMA-fed scorer's full passes, how many its
+        filter flagged, and how many of those held a passing column."""
+        a, b, c = ctypes.c_ulonglong(), ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        check(_lib.lib().snn_get_filter_counters(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"row_chunks": a.value, "flagged": b.value, "passed": c.value}
+
+    def step_timing(self):
+        """Per greedy step of the last run: (score_ms, commit_ms) arrays."""
+        n = self.p
+        sc, cm = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        k = check(_lib.lib().snn_get_step_timing(self._h, ptr(sc, _f32p), ptr(cm, _f32p), n))
+        return sc[:k], cm[:k]
+
     def timing(self):
         s, c, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         ns, nc, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
