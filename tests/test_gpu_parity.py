@@ -294,3 +294,31 @@ def test_noalloc_backward_step_matches_handle():
     best = [(err[c].min(), c, int(k_vals[int(np.argmin(err[c]))])) for c in range(p)]
     e, c, k = min(best, key=lambda t: (t[0], t[1]))
     assert (c, k) == want[:2] and e == want[2]
+
+
+@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("case", [
+    dict(n_train=300, n_val=70, p=2, kv=[3], nf=2, method="forward"),       # fewer candidates than a warp's four
+    dict(n_train=260, n_val=50, p=3, kv=[2, 5], nf=1, method="backward"),
+    dict(n_train=37, n_val=29, p=4, kv=[6, 1], nf=3, method="forward"),      # less than one 64-column chunk
+    dict(n_train=20, n_val=13, p=5, kv=[30, 3], nf=2, method="forward"),     # k > training rows: padded lists
+    dict(n_train=25, n_val=9, p=4, kv=[28], nf=2, method="backward"),
+])
+def test_edge_shapes_match_oracle(case, kernel):
+    rng = np.random.default_rng(case["n_train"] * 7 + case["p"])
+    Xt = rng.normal(size=(case["n_train"], case["p"])).astype(np.float32)
+    Xv = rng.normal(size=(case["n_val"], case["p"])).astype(np.float32)
+    yt = (Xt[:, 0] - 0.5 * Xt[:, -1] + rng.normal(0, 0.1, case["n_train"])).astype(np.float32)
+    yv = (Xv[:, 0] - 0.5 * Xv[:, -1] + rng.normal(0, 0.1, case["n_val"])).astype(np.float32)
+    if kernel == 3 and max(case["kv"]) > 32:
+        pytest.skip("the TMA-fed kernel handles k_max <= 32")
+    prob = oracle.Problem(Xt, yt, Xv, yv)
+    o = oracle.select(prob, case["kv"], case["nf"], case["method"])
+    with Selector(Xt, yt, Xv, yv, k_vals=case["kv"], num_features=case["nf"], method=case["method"]) as sel:
+        sel.set_kernel(kernel)
+        r = sel.run()
+    np.testing.assert_array_equal(r["ordering"], o["ordering"])
+    np.testing.assert_array_equal(r["mask"], o["mask"])
+    np.testing.assert_array_equal(r["errors"], o["errors"])
+    np.testing.assert_array_equal(r["step_best_k"], o["step_best_k"])
+    assert r["best_k"] == o["best_k"] and r["num_final"] == o["num_final"]
