@@ -392,7 +392,8 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     const int rg = w / (kCandB / kCW), cw = w % (kCandB / kCW);
     const int wr0 = r0 + rg * kRW;
     const int wc = cw * kCW;
-    const bool wvalid = wr0 < b.n_rows;
+    // a warp whose rows or candidate slots are all padding only releases stages
+    const bool wvalid = wr0 < b.n_rows && c0 + wc < n_cand;
     float *myL = S.Lds + w * kP * KL;
     int *myI = S.Lis + w * kP * KL;
     float *myT = S.thr_s + w * kP;
