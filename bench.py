@@ -78,9 +78,9 @@ def job_value(evals_per_rank, ms_max, world):
 
 def scoring_kernel(kmax, option=0):
     """Name of the full-scan scoring kernel the library picks (option 0 = automatic)."""
-    if option == 3 or (option == 0 and kmax <= 32):
+    if option == 3 or (option == 0 and kmax <= 64):
         return "k_score_tma"
-    if option == 2 or (option == 0 and kmax <= 64):
+    if option == 2:
         return "k_score_rw"
     return "k_score"
 
@@ -509,7 +509,7 @@ def main():
                     help="scale n_train and n_val (small cases for profiler captures; not the bench workload)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiler captures)")
     ap.add_argument("--prune", type=int, default=0, help="exact pruning of forward steps (library option)")
-    ap.add_argument("--kernel", type=int, default=0, help="full-scan kernel: 0 auto, 1 rows per lane, 2 row per warp")
+    ap.add_argument("--kernel", type=int, default=0, help="full-scan kernel: 0 auto, 1 rows per lane, 2 row tiles per warp, 3 TMA-fed row tiles")
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=["fwd-64k", "bwd-50k", "fwd-200k", "batch-64x5"],
                     help="fwd-64k (the headline), bwd-50k (backward, p=120 -> 20), fwd-200k (80 GB distance matrix, "

@@ -188,9 +188,9 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
  *                  pays off only when few columns survive).  Default 0. */
 #define SNN_OPT_PRUNE 1
 /*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic (3 for
- *                  k_max <= 32, else 2 for k_max <= 64, else 1), 1 rows per
- *                  lane (any k_max <= 256), 2 row tiles per warp (k_max <= 64),
- *                  3 row tiles fed by a TMA/mbarrier ring (k_max <= 32).
+ *                  k_max <= 64, else 1), 1 rows per lane (any k_max <= 256),
+ *                  2 row tiles per warp (k_max <= 64), 3 row tiles fed by a
+ *                  TMA/mbarrier ring (k_max <= 64).
  *                  Results are identical; this exists for cross-checks and
  *                  measurement. */
 #define SNN_OPT_KERNEL 2
@@ -206,7 +206,7 @@ SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, 
 /* Tracing of the TMA-fed scorer since the last run/step/reset: (row, chunk)
  * pairs of its full passes (a chunk = 64 training columns), how many the
  * sign-bit filter flagged for exact re-scoring, and how many of those held a
- * passing column.  Kept by that scorer only (k_max <= 32) and only while
+ * passing column.  Kept by that scorer only (k_max <= 64) and only while
  * SNN_OPT_COUNTERS is set. */
 SNN_API int snn_get_filter_counters(snn_handle *h, unsigned long long *row_chunks, unsigned long long *flagged,
                                     unsigned long long *passed);

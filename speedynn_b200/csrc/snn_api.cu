@@ -762,7 +762,7 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value)
         if (value == 2 && !snn::score_rw_supported(h->kmax))
             return fail(SNN_ERR_UNSUPPORTED, "the row-tile kernel handles k_max <= 64");
         if (value == 3 && !snn::score_tma_supported(h->kmax))
-            return fail(SNN_ERR_UNSUPPORTED, "the TMA-fed kernel handles k_max <= 32");
+            return fail(SNN_ERR_UNSUPPORTED, "the TMA-fed kernel handles k_max <= 64");
         h->kernel = value;
         return SNN_OK;
     case SNN_OPT_COUNTERS: h->count_filter = value != 0; return SNN_OK;

@@ -88,7 +88,7 @@ int record_error(int code, const char *msg);
 void clear_error();
 
 // Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 32.
-bool score_tma_supported(int kmax);
+bool score_tma_supported(int kmax);  // kernel option 3: k_max <= 64
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
 
 // Row-per-warp scoring (snn_score_rw.cu), k_max <= 64.

@@ -1,11 +1,14 @@
 // snn_score_tma.cu -- candidate scoring, warp-specialised TMA pipeline.
 //
-// Contract as snn_score_rw.cu: exact top-k_max lists (k <= 32) in the
-// reference's stable (distance, index) order and kNN-mean predictions.  A
-// block scores 24 rows x 12 candidates; each of its 18 consumer warps owns 4
-// rows x 4 candidates and walks the columns two per lane with packed f32x2
-// (18 consumers + 1 producer = 19 warps, at most 5 per SM sub-partition at
-// 96 registers; 12-candidate groups leave no padded slot for 60 candidates).
+// Contract as snn_score_rw.cu: exact top-k_max lists (k <= 64) in the
+// reference's stable (distance, index) order and kNN-mean predictions.  For
+// k <= 32 a block scores 24 rows x 12 candidates; each of its 18 consumer
+// warps owns 4 rows x 4 candidates and walks the columns two per lane with
+// packed f32x2 (18 consumers + 1 producer = 19 warps, at most 5 per SM
+// sub-partition at 96 registers; 12-candidate groups leave no padded slot for
+// 60 candidates).  For 32 < k <= 64 the 64-slot lists take more shared memory
+// and registers (two entries per lane): blocks of 16 rows x 12 candidates,
+// 12 consumer warps.
 //
 //   * Feed: one producer lane streams 256-column stages into a ring of
 //     shared-memory slots (as deep as fits beside the lists): a 2-D
@@ -45,17 +48,17 @@ constexpr int kSC = 256;          // columns per stage
 constexpr int kMaxRing = 8;       // most stages in the ring (the depth is a template argument)
 constexpr int kBarBytes = 128;    // full + empty mbarriers, padded so the tiles stay 128-byte aligned
 static_assert(2 * kMaxRing * sizeof(uint64_t) <= kBarBytes, "mbarriers must fit their area");
-constexpr int kRowsB = 24;        // scored rows per block
-constexpr int kCandB = 12;        // candidates per block
-constexpr int kConsumers = 18;    // consumer warps (6 row groups x 3 candidate groups)
+// A block has RG x CG consumer warps (template arguments), each owning kRW
+// rows x kCW candidates: kRowsB = RG * kRW scored rows, kCandB = CG * kCW
+// candidates, kConsumers = RG * CG.
 constexpr int kRingDeep = 5;      // ring slots beside 16-slot lists (k <= 16)
-constexpr int kRingShallow = 4;   // ring slots beside 32-slot lists (k <= 32)
+constexpr int kRingShallow = 4;   // ring slots beside 32- and 64-slot lists
 constexpr int kRW = 4, kCW = 4, kP = kRW * kCW;
 constexpr long long kSpinLimit = 1ll << 22;  // try_wait polls before giving up
 constexpr unsigned long long kWaitNs = 1000000000ull;  // one second
 
-// Shared-memory slots per neighbour list (k <= 32).
-__host__ __device__ constexpr int list_slots(int K) { return K <= 16 ? 16 : 32; }
+// Shared-memory slots per neighbour list (k <= 64).
+__host__ __device__ constexpr int list_slots(int K) { return K <= 16 ? 16 : K <= 32 ? 32 : 64; }
 
 __device__ __forceinline__ unsigned long long as_u64(float2 v) { return *reinterpret_cast<unsigned long long *>(&v); }
 __device__ __forceinline__ float2 as_f2(unsigned long long v) { return *reinterpret_cast<float2 *>(&v); }
@@ -203,8 +206,7 @@ __device__ __forceinline__ void tma_gather4(void *dst, const CUtensorMap *map, i
 // strict test d < kth into the inclusive d <= below(kth).
 __device__ __forceinline__ float below(float x) { return x > 0.0f ? __int_as_float(__float_as_int(x) - 1) : -0x1p-149f; }
 
-// Insert a chunk's passing distances into the warp's lists (forward,
-// K <= 32).  pm holds this lane's passes, bit 2*p + h for problem p and chunk
+// Insert a chunk's passing distances into the warp's lists (K <= KL <= 64).  pm holds this lane's passes, bit 2*p + h for problem p and chunk
 // column 2*lane + h; D_s / X_s are the warp's D rows and candidate X rows of
 // the stage (kSC columns each).  Items go in column order with the reference
 // rule (after every element <= d, entry below the k-th once the list is
@@ -212,10 +214,11 @@ __device__ __forceinline__ float below(float x) { return x > 0.0f ? __int_as_flo
 // memory, and the list being filled sits in registers, lane j holding entry j.
 // Returns a mask of the warp's rows (bit p / kCW) whose thresholds may have
 // changed.
-template <bool BWD>
+template <bool BWD, int KL>
 __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, const float *X_s, const float *myX, float *myL,
-                                          int *myI, float *myT, int q0, int colbase, int K, int KL)
+                                          int *myI, float *myT, int q0, int colbase, int K)
 {
+    constexpr bool LONG = KL > 32;
     const int lane = threadIdx.x & 31;
     unsigned rows = 0u;
     unsigned any = __reduce_or_sync(kFull, pm);
@@ -224,8 +227,15 @@ __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, 
         any &= ~(3u << (2 * p));
         float *L = myL + p * KL;
         int *LI = myI + p * KL;
-        float Lj = lane < K ? L[lane] : INFINITY;
-        int Ij = lane < K ? LI[lane] : 0;
+        // lane j holds entry j (and, for k_max > 32, entry j + 32)
+        float L0 = lane < K ? L[lane] : INFINITY;
+        int I0 = lane < K ? LI[lane] : 0;
+        float L1 = INFINITY;
+        int I1 = 0;
+        if constexpr (LONG) {
+            L1 = lane + 32 < K ? L[lane + 32] : INFINITY;
+            I1 = lane + 32 < K ? LI[lane + 32] : 0;
+        }
         float th = myT[p];
         const float xv = myX[p];
         const float *xrow = X_s + (p % kCW) * kSC + q0;
@@ -244,24 +254,51 @@ __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, 
                 const float d = BWD ? __fsub_rn(dr[c], s1) : __fadd_rn(dr[c], s1);
                 if (d <= th) {
                     // d < FLT_MAX and, for a full list, d < k-th: the slot is < K
-                    const int pos = __popc(__ballot_sync(kFull, lane < K && Lj <= d));
-                    const float upL = __shfl_up_sync(kFull, Lj, 1);
-                    const int upI = __shfl_up_sync(kFull, Ij, 1);
-                    if (lane == pos) {
-                        Lj = d;
-                        Ij = colbase + c;
-                    } else if (lane > pos) {
-                        Lj = upL;
-                        Ij = upI;
+                    int pos = __popc(__ballot_sync(kFull, lane < K && L0 <= d));
+                    const float up0 = __shfl_up_sync(kFull, L0, 1);
+                    const int upi0 = __shfl_up_sync(kFull, I0, 1);
+                    if constexpr (LONG) {
+                        pos += __popc(__ballot_sync(kFull, lane + 32 < K && L1 <= d));
+                        // entry 31 moves to entry 32 (lane 0 of the second half)
+                        float up1 = __shfl_up_sync(kFull, L1, 1);
+                        int upi1 = __shfl_up_sync(kFull, I1, 1);
+                        const float c31 = __shfl_sync(kFull, L0, 31);
+                        const int ci31 = __shfl_sync(kFull, I0, 31);
+                        if (lane == 0) {
+                            up1 = c31;
+                            upi1 = ci31;
+                        }
+                        if (lane + 32 == pos) {
+                            L1 = d;
+                            I1 = colbase + c;
+                        } else if (lane + 32 > pos) {
+                            L1 = up1;
+                            I1 = upi1;
+                        }
                     }
-                    const float kth = __shfl_sync(kFull, Lj, K - 1);
+                    if (lane == pos) {
+                        L0 = d;
+                        I0 = colbase + c;
+                    } else if (lane > pos) {
+                        L0 = up0;
+                        I0 = upi0;
+                    }
+                    float kth;
+                    if constexpr (LONG) kth = K <= 32 ? __shfl_sync(kFull, L0, (K - 1) & 31) : __shfl_sync(kFull, L1, (K - 33) & 31);
+                    else kth = __shfl_sync(kFull, L0, K - 1);
                     if (kth < FLT_MAX) th = BWD ? nextafterf(kth, -INFINITY) : below(kth);
                 }
             }
         }
         if (lane < K) {
-            L[lane] = Lj;
-            LI[lane] = Ij;
+            L[lane] = L0;
+            LI[lane] = I0;
+        }
+        if constexpr (LONG) {
+            if (lane + 32 < K) {
+                L[lane + 32] = L1;
+                LI[lane + 32] = I1;
+            }
         }
         if (lane == 0) myT[p] = th;
         rows |= 1u << (p / kCW);
@@ -294,8 +331,10 @@ struct TmaSmem {
     int *flag;
 };
 
+template <int RG, int CG>
 __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL, int ring)
 {
+    constexpr int kRowsB = RG * kRW, kCandB = CG * kCW, kConsumers = RG * CG;
     TmaSmem S;
     uint64_t *bars = reinterpret_cast<uint64_t *>(base);
     S.full = bars;
@@ -313,14 +352,20 @@ __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL, int ri
     return S;
 }
 
-template <bool BWD, int ring, bool COUNT>
-__global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg, const __grid_constant__ CUtensorMap tmD,
-                                                                   const __grid_constant__ CUtensorMap tmX)
+// RG x CG consumer warps (row groups x candidate groups of 4); KL list slots
+// per row (16, 32 or 64).  KL = 64 (k_max in (32, 64]) keeps two list entries
+// and two first-pass minima per lane.
+// (32, 64] -- two list entries per lane and two first-pass minima per lane.
+template <bool BWD, int ring, bool COUNT, int RG, int CG, int KL>
+__global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg,
+                                                                     const __grid_constant__ CUtensorMap tmD,
+                                                                     const __grid_constant__ CUtensorMap tmX)
 {
+    constexpr int kRowsB = RG * kRW, kCandB = CG * kCW, kConsumers = RG * CG;
     extern __shared__ __align__(128) unsigned char smraw[];
     const int K = b.kmax;
-    const int KL = list_slots(K);
-    const TmaSmem S = carve_tma(smraw, KL, ring);
+    constexpr bool LONG = KL > 32;
+    const TmaSmem S = carve_tma<RG, CG>(smraw, KL, ring);
     if (b.st->done) return;
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -438,10 +483,12 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     // the exact distance; forward takes a = fl(t*t + D) (one FMA), which is at
     // most 3 ulp below the exact d = fl(D + fl(t*t)) for D >= 0, so the bound
     // derived from it is widened by 2^-20 relative (see fwd_bound).
+    // For k_max > 32 each lane keeps two minima (its even and its odd columns),
+    // 64 values from distinct columns.
     {
-        float mn[kP];
+        float mn[kP], mn2[kP];  // mn2: LONG only
 #pragma unroll
-        for (int p = 0; p < kP; ++p) mn[p] = INFINITY;
+        for (int p = 0; p < kP; ++p) mn[p] = mn2[p] = INFINITY;
         for (int v = 0; v < nA && alive; ++v) {
             const int s = v % ring;
             if (!mbar_wait(S.full + s, (v / ring) & 1)) {
@@ -469,18 +516,33 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                             float2 e;
                             if constexpr (BWD) e = sub2(dp[ri], sq2(t));
                             else e = fma2(t, t, dp[ri]);
-                            mn[p] = min3f(mn[p], e.x, e.y);
+                            if constexpr (LONG) {
+                                mn[p] = fminf(mn[p], e.x);
+                                mn2[p] = fminf(mn2[p], e.y);
+                            } else {
+                                mn[p] = min3f(mn[p], e.x, e.y);
+                            }
                         }
                 }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(S.empty + s);
         }
-        // T = k-th smallest of the 32 lane minima (k <= 32): k distinct columns lie at or below it
+        // T = k-th smallest of the 32 (64) lane minima: k distinct columns lie at or below it
 #pragma unroll
         for (int p = 0; p < kP; ++p) {
-            const float srt = warp_sort32(mn[p], lane);
-            const float T = __shfl_sync(kFull, srt, (K - 1) & 31);
+            float T;
+            if constexpr (LONG) {
+                // both halves sorted, the second reversed: element-wise min / max split
+                // the 64 values into the 32 smallest and the 32 largest
+                const float a = warp_sort32(mn[p], lane);
+                const float bz = __shfl_sync(kFull, warp_sort32(mn2[p], lane), 31 - lane);
+                const float lo = warp_sort32(fminf(a, bz), lane), hi = warp_sort32(fmaxf(a, bz), lane);
+                T = K <= 32 ? __shfl_sync(kFull, lo, (K - 1) & 31) : __shfl_sync(kFull, hi, (K - 33) & 31);
+            } else {
+                const float srt = warp_sort32(mn[p], lane);
+                T = __shfl_sync(kFull, srt, K - 1);
+            }
             float th;
             if constexpr (BWD) {
                 float Tb = T;
@@ -585,7 +647,7 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
                         }
                         if (__any_sync(kFull, pm != 0u)) {
                             const unsigned rows =
-                                insert_chunk<BWD>(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K, KL);
+                                insert_chunk<BWD, KL>(pm, D_s, X_s, myX, myL, myI, myT, q0, i0 + q0, K);
 #pragma unroll
                             for (int ri = 0; ri < kRW; ++ri)
                                 if ((rows >> ri) & 1u) H2[ri] = row_H(ri);
@@ -652,9 +714,10 @@ __global__ void __launch_bounds__((kConsumers + 1) * 32, 1) k_score_tma(Bufs b, 
     }
 }
 
-size_t tma_smem_bytes(int K, int ring)
+size_t tma_smem_bytes(int K, int ring, int RG, int CG)
 {
     const int KL = list_slots(K);
+    const int kRowsB = RG * kRW, kCandB = CG * kCW, kConsumers = RG * CG;
     return kBarBytes + sizeof(float) * (size_t)ring * (kRowsB + kCandB) * kSC +
            (sizeof(float) + sizeof(int)) * (size_t)kConsumers * kP * KL + 2 * sizeof(float) * kConsumers * kP +
            sizeof(int) * (kCandB + 1 + 2 * kConsumers);
@@ -662,7 +725,7 @@ size_t tma_smem_bytes(int K, int ring)
 
 }  // namespace
 
-bool score_tma_supported(int kmax) { return kmax >= 1 && kmax <= 32; }
+bool score_tma_supported(int kmax) { return kmax >= 1 && kmax <= 64; }
 
 namespace {
 
@@ -698,32 +761,53 @@ bool encode_rows(CUtensorMap *m, const float *base, int ld, long long rows, int 
 
 }  // namespace
 
-cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s)
+namespace {
+
+template <bool BWD, bool COUNT, int RING, int RG, int CG, int KL>
+cudaError_t launch_shape(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 {
+    constexpr int kRowsB = RG * kRW, kCandB = CG * kCW;
     const int n_cg = (n_cand + kCandB - 1) / kCandB;
     const long long blocks = (long long)((b.n_rows + kRowsB - 1) / kRowsB) * n_cg;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     CUtensorMap tmD, tmX;
     if (!encode_rows(&tmD, b.D, b.ldc, b.n_rows, kRowsB) || !encode_rows(&tmX, b.XT, b.ldc, b.p, 1))
         return cudaErrorInvalidValue;
-    // ring depth: as many 32 KB stages as fit beside the lists (16 or 32 slots)
+    const size_t smem = tma_smem_bytes(b.kmax, RING, RG, CG);
+    if (smem > (size_t)max_smem) return cudaErrorInvalidConfiguration;
+    if (list_slots(b.kmax) != KL) return cudaErrorInvalidValue;
+    auto kern = k_score_tma<BWD, RING, COUNT, RG, CG, KL>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<(unsigned)blocks, (RG * CG + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);
+    return cudaGetLastError();
+}
+
+template <bool BWD, bool COUNT>
+cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
+{
+    // 16-slot lists leave room for a 5-slot ring of 24-row x 12-candidate stages,
+    // 32-slot lists for 4 slots; 64-slot lists (k <= 64) take 16-row x
+    // 12-candidate blocks (12 consumer warps) to keep 4 ring slots.
+    switch (list_slots(b.kmax)) {
+    case 16: return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, max_smem, s);
+    case 32: return launch_shape<BWD, COUNT, kRingShallow, 6, 3, 32>(b, n_cand, max_smem, s);
+    default: return launch_shape<BWD, COUNT, kRingShallow, 4, 3, 64>(b, n_cand, max_smem, s);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s)
+{
     int dev = 0, max_smem = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
-    const bool deep = list_slots(b.kmax) == 16;
-    const size_t smem = tma_smem_bytes(b.kmax, deep ? kRingDeep : kRingShallow);
-    if (smem > (size_t)max_smem) return cudaErrorInvalidConfiguration;
     // the counting variants are separate instantiations: the default code has no counting at all
     const bool cnt = b.fcount != nullptr;
-    auto kern = backward ? (deep ? (cnt ? k_score_tma<true, kRingDeep, true> : k_score_tma<true, kRingDeep, false>)
-                                 : (cnt ? k_score_tma<true, kRingShallow, true> : k_score_tma<true, kRingShallow, false>))
-                         : (deep ? (cnt ? k_score_tma<false, kRingDeep, true> : k_score_tma<false, kRingDeep, false>)
-                                 : (cnt ? k_score_tma<false, kRingShallow, true> : k_score_tma<false, kRingShallow, false>));
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<(unsigned)blocks, (kConsumers + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);
-    return cudaGetLastError();
+    if (backward) return cnt ? launch_k<true, true>(b, n_cand, max_smem, s) : launch_k<true, false>(b, n_cand, max_smem, s);
+    return cnt ? launch_k<false, true>(b, n_cand, max_smem, s) : launch_k<false, false>(b, n_cand, max_smem, s);
 }
 
 }  // namespace snn

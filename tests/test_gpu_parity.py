@@ -109,14 +109,16 @@ def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, kernel=0, **kw):
     (400, 130, 9, 11, [150, 2], 2, "backward"),        # k_max 150 -> 1 per thread
     (1290, 410, 11, 12, [17, 2], 5, "forward"),        # 32-slot lists; last 256-column stage holds one chunk
     (830, 300, 10, 13, [20], 6, "backward"),           # backward with 32-slot lists
+    (1100, 333, 13, 14, [50, 33, 3], 5, "forward"),    # 64-slot lists, k_max 50
+    (900, 250, 11, 15, [40], 5, "backward"),           # backward with 64-slot lists
 ])
 @pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_holdout_matches_oracle(args, kernel):
     n_train, n_val, p, seed, kv, nf, method = args
     if kernel == 2 and max(kv) > 64:
         pytest.skip("the row-tile kernel handles k_max <= 64")
-    if kernel == 3 and max(kv) > 32:
-        pytest.skip("the TMA-fed kernel handles k_max <= 32")
+    if kernel == 3 and max(kv) > 64:
+        pytest.skip("the TMA-fed kernel handles k_max <= 64")
     o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method, kernel=kernel)
     np.testing.assert_array_equal(r["ordering"], o["ordering"])
     np.testing.assert_array_equal(r["mask"], o["mask"])
@@ -303,6 +305,8 @@ def test_noalloc_backward_step_matches_handle():
     dict(n_train=37, n_val=29, p=4, kv=[6, 1], nf=3, method="forward"),      # less than one 64-column chunk
     dict(n_train=20, n_val=13, p=5, kv=[30, 3], nf=2, method="forward"),     # k > training rows: padded lists
     dict(n_train=25, n_val=9, p=4, kv=[28], nf=2, method="backward"),
+    dict(n_train=45, n_val=11, p=4, kv=[50, 2], nf=2, method="forward"),     # 64-slot lists, k > training rows
+    dict(n_train=70, n_val=17, p=3, kv=[33], nf=2, method="backward"),
 ])
 def test_edge_shapes_match_oracle(case, kernel):
     rng = np.random.default_rng(case["n_train"] * 7 + case["p"])
@@ -310,8 +314,8 @@ def test_edge_shapes_match_oracle(case, kernel):
     Xv = rng.normal(size=(case["n_val"], case["p"])).astype(np.float32)
     yt = (Xt[:, 0] - 0.5 * Xt[:, -1] + rng.normal(0, 0.1, case["n_train"])).astype(np.float32)
     yv = (Xv[:, 0] - 0.5 * Xv[:, -1] + rng.normal(0, 0.1, case["n_val"])).astype(np.float32)
-    if kernel == 3 and max(case["kv"]) > 32:
-        pytest.skip("the TMA-fed kernel handles k_max <= 32")
+    if kernel == 3 and max(case["kv"]) > 64:
+        pytest.skip("the TMA-fed kernel handles k_max <= 64")
     prob = oracle.Problem(Xt, yt, Xv, yv)
     o = oracle.select(prob, case["kv"], case["nf"], case["method"])
     with Selector(Xt, yt, Xv, yv, k_vals=case["kv"], num_features=case["nf"], method=case["method"]) as sel:
