@@ -326,3 +326,29 @@ def test_edge_shapes_match_oracle(case, kernel):
     np.testing.assert_array_equal(r["errors"], o["errors"])
     np.testing.assert_array_equal(r["step_best_k"], o["step_best_k"])
     assert r["best_k"] == o["best_k"] and r["num_final"] == o["num_final"]
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_forward_bound_overflow_and_ties(kernel):
+    """Forward steps after the first bound each list by its last neighbours'
+    distances under the new D.  A dominant feature whose squared differences
+    overflow to inf (selected first) leaves those distances non-finite, so the
+    bound falls back to none; quantized values give ties at the bound."""
+    rng = np.random.default_rng(77)
+    n_train, n_val, p = 900, 260, 7
+    Xt = rng.integers(-3, 4, size=(n_train, p)).astype(np.float32)
+    Xv = rng.integers(-3, 4, size=(n_val, p)).astype(np.float32)
+    Xt[:, 2] *= np.float32(1e19)
+    Xv[:, 2] *= np.float32(1e19)
+    yt = (np.sign(Xt[:, 2]) + 0.3 * Xt[:, 0] + rng.normal(0, 0.05, n_train)).astype(np.float32)
+    yv = (np.sign(Xv[:, 2]) + 0.3 * Xv[:, 0] + rng.normal(0, 0.05, n_val)).astype(np.float32)
+    prob = oracle.Problem(Xt, yt, Xv, yv)
+    o = oracle.select(prob, [1, 6, 21], 4, "forward")
+    with Selector(Xt, yt, Xv, yv, k_vals=[1, 6, 21], num_features=4, method="forward") as sel:
+        sel.set_kernel(kernel)
+        r = sel.run()
+    assert o["ordering"][0] == 2
+    np.testing.assert_array_equal(r["ordering"], o["ordering"])
+    np.testing.assert_array_equal(r["errors"], o["errors"])
+    np.testing.assert_array_equal(r["step_best_k"], o["step_best_k"])
+    assert r["best_k"] == o["best_k"] and r["num_final"] == o["num_final"]
