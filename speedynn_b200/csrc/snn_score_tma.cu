@@ -6,9 +6,8 @@
 // warps owns 4 rows x 4 candidates and walks the columns two per lane with
 // packed f32x2 (18 consumers + 1 producer = 19 warps, at most 5 per SM
 // sub-partition at 96 registers; 12-candidate groups leave no padded slot for
-// 60 candidates).  For 32 < k <= 64 the 64-slot lists take more shared memory
-// and registers (two entries per lane): blocks of 16 rows x 12 candidates,
-// 12 consumer warps.
+// 60 candidates).  For 32 < k <= 64 the 64-slot lists (two entries per lane)
+// take more shared memory: the same blocks with a 2-slot ring.
 //
 //   * Feed: one producer lane streams 256-column stages into a ring of
 //     shared-memory slots (as deep as fits beside the lists): a 2-D
@@ -786,13 +785,14 @@ cudaError_t launch_shape(const Bufs &b, int n_cand, int max_smem, cudaStream_t s
 template <bool BWD, bool COUNT>
 cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 {
-    // 16-slot lists leave room for a 5-slot ring of 24-row x 12-candidate stages,
-    // 32-slot lists for 4 slots; 64-slot lists (k <= 64) take 16-row x
-    // 12-candidate blocks (12 consumer warps) to keep 4 ring slots.
+    // 24-row x 12-candidate blocks throughout: 16-slot lists leave room for a
+    // 5-slot ring, 32-slot lists for 4 slots, 64-slot lists (k <= 64) for 2
+    // (measured on k = 50: 19 warps with 2 slots beat 16 warps with 3 and 13
+    // warps with 4).
     switch (list_slots(b.kmax)) {
     case 16: return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, max_smem, s);
     case 32: return launch_shape<BWD, COUNT, kRingShallow, 6, 3, 32>(b, n_cand, max_smem, s);
-    default: return launch_shape<BWD, COUNT, kRingShallow, 4, 3, 64>(b, n_cand, max_smem, s);
+    default: return launch_shape<BWD, COUNT, 2, 6, 3, 64>(b, n_cand, max_smem, s);
     }
 }
 
