@@ -250,9 +250,12 @@ SNN_API int snn_batch_run(snn_batch *b);
 SNN_API int snn_batch_get_results(snn_batch *b, int i, int *ordering, int *mask, float *errors, double *errors64,
                                   int *step_best_k, int *best_k, int *num_final);
 
-/* Wall time of the last snn_batch_run spent running waves (from the first
- * launch of a wave to its last result; creating and loading excluded), and
- * the number of waves. */
+/* Device time of the last snn_batch_run's selections, and the number of
+ * waves.  Each problem's selection is issued on its stream as soon as the
+ * problem is created and loaded, so later creates and uploads overlap earlier
+ * selections; run_ms is the union, over waves, of the intervals in which some
+ * selection of the wave was running (CUDA events around each problem's greedy
+ * steps; creating, loading and reading results are outside them). */
 SNN_API int snn_batch_get_timing(snn_batch *b, double *run_ms, int *waves);
 
 SNN_API int snn_batch_destroy(snn_batch *b);

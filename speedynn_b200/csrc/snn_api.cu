@@ -14,7 +14,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <chrono>
 #include <string>
 #include <vector>
 
@@ -851,20 +850,25 @@ struct snn_batch {
 
 namespace {
 
-// Run problems [i0, i1) of the batch, all created and loaded: every selection
-// is issued on its handle's own stream before any result is read, so the
-// problems overlap on the GPU.
-int run_wave(snn_batch *B, std::vector<snn_handle *> &hs, int i0)
+// Issue a loaded batch problem's whole selection on its own stream, between
+// its total_ev events (snn_load has just reset it), without waiting.
+int issue_batch_problem(snn_handle *h)
 {
-    const auto t0 = std::chrono::steady_clock::now();
-    for (snn_handle *h : hs) {
-        if (cudaSetDevice(h->device) != cudaSuccess) return fail(SNN_ERR_CUDA, "cudaSetDevice failed");
-        reset_timing(h);
-        if (int rc = issue_reset(h)) return rc;
-        for (int t = 0; t < h->total_steps; ++t)
-            if (int rc = issue_step(h, t)) return rc;
-        h->host_step = h->total_steps;
-    }
+    reset_timing(h);
+    SNN_CUDA(cudaEventRecord(h->total_ev.a, h->stream));
+    for (int t = 0; t < h->total_steps; ++t)
+        if (int rc = issue_step(h, t)) return rc;
+    h->host_step = h->total_steps;
+    SNN_CUDA(cudaEventRecord(h->total_ev.b, h->stream));
+    return SNN_OK;
+}
+
+// Collect the results of problems [i0, i0 + hs.size()) of the batch, all
+// issued, and add the wave's device time: the union of the problems' event
+// intervals (the GPU ran some selection of the wave throughout it).
+int finish_wave(snn_batch *B, std::vector<snn_handle *> &hs, int i0)
+{
+    std::vector<std::pair<float, float>> iv;
     for (size_t j = 0; j < hs.size(); ++j) {
         snn_handle *h = hs[j];
         snn_batch::Problem &P = B->prob[i0 + j];
@@ -881,8 +885,24 @@ int run_wave(snn_batch *B, std::vector<snn_handle *> &hs, int i0)
         if (int rc = snn_get_results(h, P.ordering.data(), P.mask.data(), P.err.data(), P.err64.data(), P.stepk.data(),
                                      &P.best_k, &P.num_final))
             P.status = rc;
+        float a = 0.0f, b = 0.0f;  // relative to the first problem's start event
+        SNN_CUDA(cudaEventElapsedTime(&a, hs[0]->total_ev.a, h->total_ev.a));
+        SNN_CUDA(cudaEventElapsedTime(&b, hs[0]->total_ev.a, h->total_ev.b));
+        iv.emplace_back(a, b);
     }
-    B->run_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::sort(iv.begin(), iv.end());
+    double busy = 0.0, lo = 0.0, hi = 0.0;
+    for (size_t j = 0; j < iv.size(); ++j) {
+        if (j == 0 || iv[j].first > hi) {
+            busy += hi - lo;
+            lo = iv[j].first;
+            hi = iv[j].second;
+        } else {
+            hi = std::max<double>(hi, iv[j].second);
+        }
+    }
+    busy += hi - lo;
+    B->run_ms += busy;
     B->waves++;
     return SNN_OK;
 }
@@ -972,8 +992,10 @@ SNN_API int snn_batch_run(snn_batch *B)
             hs.push_back(h);
             used += need;
             ++i;
+            // start this problem now: later creates and uploads overlap its steps
+            if ((rc = issue_batch_problem(h))) break;
         }
-        if (rc == SNN_OK && !hs.empty()) rc = run_wave(B, hs, i0);
+        if (rc == SNN_OK && !hs.empty()) rc = finish_wave(B, hs, i0);
         for (snn_handle *h : hs) snn_destroy(h);
         if (rc) return fail(rc, "snn_batch_run, problem %d: %s", i, std::string(g_err).c_str());
     }
