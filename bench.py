@@ -447,6 +447,25 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_plain(probs, batch_res, evals, batch_ms, world):
+    """The plain single-problem form of the batch workload: the same problems
+    one after another through the handle API (device time of each snn_run),
+    with the selected features and errors checked against the batch's."""
+    from speedynn_b200.selector import Selector
+
+    plain_ms = 0.0
+    same = True
+    for pr, rb in zip(probs, batch_res):
+        with Selector(pr["Xtrain"], pr["ytrain"], pr["Xval"], pr["yval"], k_vals=pr["k_vals"],
+                      num_features=pr["num_features"], method=pr["method"]) as sel:
+            r = sel.run()
+            plain_ms += sel.timing()["total_ms"]
+        same = same and np.array_equal(r["ordering"], rb["ordering"]) and np.array_equal(r["errors"], rb["errors"])
+    return {"ms": plain_ms, "value": world * evals / (plain_ms / 1000.0), "batched_speedup": plain_ms / batch_ms,
+            "identical_results": bool(same),
+            "note": "the problems one at a time (CUDA-event time of each selection, creates and uploads excluded)"}
+
+
 def run_batch(args, world, rank, local):
     """One bench step = one snn_batch_run over the 320 holdout problems of the
     batch workload (64 pools x 5 seeded train/validation splits)."""
@@ -470,7 +489,7 @@ def run_batch(args, world, rank, local):
     waves = 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        b.run()
+        res = b.run()
         wall += time.perf_counter() - t0
         tm = b.timing()
         run_ms += tm["run_ms"]
@@ -491,6 +510,8 @@ def run_batch(args, world, rank, local):
             "e2e": {"value": world * evals / (wall / args.steps), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(sum(pr["Xtrain"].shape[1] * 28 + 8 for pr in probs))},
             "clocks": clocks}
+    if not args.no_plain and args.steps > 0:
+        line["plain"] = run_plain(probs, res, evals, ms, world)
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -508,6 +529,8 @@ def main():
     ap.add_argument("--rows-scale", type=float, default=1.0,
                     help="scale n_train and n_val (small cases for profiler captures; not the bench workload)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiler captures)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="batch workload: skip running the problems one at a time for comparison")
     ap.add_argument("--prune", type=int, default=0, help="exact pruning of forward steps (library option)")
     ap.add_argument("--kernel", type=int, default=0, help="full-scan kernel: 0 auto, 1 rows per lane, 2 row tiles per warp, 3 TMA-fed row tiles")
     ap.add_argument("--workload", default=WORKLOAD,

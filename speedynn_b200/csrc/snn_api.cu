@@ -463,7 +463,11 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->fcount, 3, "filter counters"))) return bail(rc);
     h->M = d->backward ? 0 : snn::seeds_for_k(kmax);
     if (h->M > 0 && (rc = dev_alloc(&h->seeds, (size_t)h->n_rows * h->M, "seed columns"))) return bail(rc);
-    if (cudaMemcpy(h->kv, h->kvals.data(), sizeof(int) * h->nk, cudaMemcpyHostToDevice) != cudaSuccess)
+    // On the handle's stream, so every kernel that reads k_vals comes after it
+    // (the source lives as long as the handle).  A cudaMemcpy here would run on
+    // the legacy stream, which does not order the handle's non-blocking stream,
+    // and from pageable memory it may return before its DMA lands.
+    if (cudaMemcpyAsync(h->kv, h->kvals.data(), sizeof(int) * h->nk, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
         return bail(fail(SNN_ERR_CUDA, "copy of k_vals failed"));
     if (make_pair(h->total_ev)) return bail(SNN_ERR_CUDA);
     t_fail_alloc = 0;
@@ -654,7 +658,10 @@ SNN_API int snn_set_model(snn_handle *h, const int *loss_ids, int n_losses, int 
         if (int rc = dev_alloc(&h->d_loss_ids, nl, "loss ids")) return rc;
         if (int rc = dev_alloc(&h->lossval, nl * p * h->nk, "losses")) return rc;
         if (int rc = dev_alloc(&h->err_all, nl * p, "losses per step")) return rc;
-        SNN_CUDA(cudaMemcpy(h->d_loss_ids, loss_ids, sizeof(int) * nl, cudaMemcpyHostToDevice));
+        // on the handle's stream (see the k_vals copy in snn_create); the wait lets
+        // the caller reuse loss_ids at once
+        SNN_CUDA(cudaMemcpyAsync(h->d_loss_ids, h->loss_ids.data(), sizeof(int) * nl, cudaMemcpyHostToDevice, h->stream));
+        SNN_CUDA(cudaStreamSynchronize(h->stream));
     }
     if (model_type == 1 && !h->nn_idx) {
         const size_t n = p * h->n_rows * h->kmax;

@@ -46,3 +46,23 @@ def test_batch_matches_single_runs(max_bytes):
     for w, g in zip(want, got):
         for k in KEYS:
             np.testing.assert_array_equal(np.asarray(g[k]), np.asarray(w[k]), err_msg=k)
+
+
+def test_many_concurrent_problems_match_single_runs():
+    """64 problems issued while later ones are still being created and loaded,
+    so early selections run on a busy GPU: every problem still equals its own
+    single-handle run (each handle's k values reach the device before its
+    first step)."""
+    rng = np.random.default_rng(9)
+    probs = []
+    for i in range(64):
+        nt = int(rng.integers(1500, 12000))
+        s = datagen.generate(nt, nt // 2, 20, n_mag=5, seed=900 + i)
+        probs.append(dict(Xtrain=s.Xtrain, ytrain=s.ytrain, Xval=s.Xval, yval=s.yval,
+                          k_vals=[[1, 5, 10, 20][i % 4]], num_features=6, method="forward"))
+    with Batch(probs) as b:
+        got = b.run()
+    for i, (pr, g) in enumerate(zip(probs, got)):
+        w = _alone(pr)
+        for k in KEYS:
+            np.testing.assert_array_equal(np.asarray(g[k]), np.asarray(w[k]), err_msg=f"problem {i}: {k}")
