@@ -87,7 +87,7 @@ constexpr int kErrTimeout = -7;  // SNN_ERR_TIMEOUT: a bounded device wait gave 
 int record_error(int code, const char *msg);
 void clear_error();
 
-// Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 32.
+// Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 64.
 bool score_tma_supported(int kmax);  // kernel option 3: k_max <= 64
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
 

@@ -1,13 +1,13 @@
 // snn_score_tma.cu -- candidate scoring, warp-specialised TMA pipeline.
 //
 // Contract as snn_score_rw.cu: exact top-k_max lists (k <= 64) in the
-// reference's stable (distance, index) order and kNN-mean predictions.  For
-// k <= 32 a block scores 24 rows x 12 candidates; each of its 18 consumer
-// warps owns 4 rows x 4 candidates and walks the columns two per lane with
-// packed f32x2 (18 consumers + 1 producer = 19 warps, at most 5 per SM
-// sub-partition at 96 registers; 12-candidate groups leave no padded slot for
-// 60 candidates).  For 32 < k <= 64 the 64-slot lists (two entries per lane)
-// take more shared memory: the same blocks with a 2-slot ring.
+// reference's stable (distance, index) order and kNN-mean predictions.  A
+// block scores 24 rows x 12 candidates; each of its 18 consumer warps owns 4
+// rows x 4 candidates and walks the columns two per lane with packed f32x2
+// (18 consumers + 1 producer = 19 warps, at most 5 per SM sub-partition at 96
+// registers; 12-candidate groups leave no padded slot for 60 candidates).
+// For 32 < k <= 64 the 64-slot lists (two entries per lane) take more shared
+// memory, which leaves room for a 2-slot ring.
 //
 //   * Feed: one producer lane streams 256-column stages into a ring of
 //     shared-memory slots (as deep as fits beside the lists): a 2-D
