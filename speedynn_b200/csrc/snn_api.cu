@@ -376,6 +376,7 @@ static size_t handle_bytes(const snn_desc *d, int kmax)
     const size_t M = d->backward ? 0 : (size_t)snn::seeds_for_k(kmax);
     size_t f = p * ldc + n_rows * ldc + p * (size_t)d->num_k_vals * n_rows + p * n_cols + std::max(n_rows, n_cols) * p +
                n_rows * M + n_cols + n_rows;
+    if (d->backward) f += p * n_rows + n_rows;  // kth_prev, dmax
     if (!cv) f += p * ldr;
     return sizeof(float) * f + ((size_t)1 << 20);
 }
