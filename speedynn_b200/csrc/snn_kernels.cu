@@ -360,13 +360,13 @@ __global__ void k_feature_variance(Bufs b, float *var)
 
 int sm_count()
 {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0;
+    // initialised once, thread-safely (handles may be created from several threads)
+    static const int n = [] {
+        int dev = 0, c = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        return c > 0 ? c : 148;
+    }();
     return n;
 }
 

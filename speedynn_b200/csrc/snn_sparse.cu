@@ -351,13 +351,13 @@ __global__ void __launch_bounds__(256) k_score_sparse(Bufs b, SparseBufs sp, int
 
 int sm_count_sp()
 {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0;
+    // initialised once, thread-safely (handles may be created from several threads)
+    static const int n = [] {
+        int dev = 0, c = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        return c > 0 ? c : 148;
+    }();
     return n;
 }
 
