@@ -352,3 +352,30 @@ def test_forward_bound_overflow_and_ties(kernel):
     np.testing.assert_array_equal(r["errors"], o["errors"])
     np.testing.assert_array_equal(r["step_best_k"], o["step_best_k"])
     assert r["best_k"] == o["best_k"] and r["num_final"] == o["num_final"]
+
+
+@pytest.mark.parametrize("method", ["forward", "backward"])
+def test_resume_from_committed_prefix_equals_uninterrupted_run(method):
+    """Checkpoint / resume: committing the first winners of a run (warm start)
+    and stepping on reproduces the rest of that run bit for bit."""
+    s = datagen.generate(3000, 1200, 16, n_mag=6, n_heavy=3, seed=61)
+    kw = dict(k_vals=[3, 9], num_features=7 if method == "forward" else 4, method=method)
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, **kw) as sel:
+        full = sel.run()
+    p = s.Xtrain.shape[1]
+    n_steps = kw["num_features"] if method == "forward" else p - kw["num_features"]
+    # winners in commit order: forward fills slots from the front, backward from the back
+    slots = list(range(n_steps)) if method == "forward" else [p - 1 - t for t in range(n_steps)]
+    winners = [int(full["ordering"][i]) for i in slots]
+    cut = 3
+    with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, **kw) as sel:
+        sel.commit_sequence(winners[:cut])
+        while sel.step():
+            pass
+        res = sel.results()
+    for i in slots[cut:]:
+        assert res["ordering"][i] == full["ordering"][i]
+        assert res["errors"][i] == full["errors"][i]
+        assert res["errors64"][i] == full["errors64"][i]
+        assert res["step_best_k"][i] == full["step_best_k"][i]
+    np.testing.assert_array_equal(res["mask"], full["mask"])
