@@ -14,7 +14,7 @@ ours:       inputs resident in HBM; each step = snn_run (initial distance
             events on the library's stream.  `e2e` repeats it through the
             public API from pinned host buffers (upload + run + result read).
 reference:  speedynn's own CPU neighbour scan (get_k_nearest_neighbors_cpu,
-            speedynn/lib/cpu.c:212-252, compiled from the reference sources
+            speedynn/lib/cpu.c:128-168, compiled from the reference sources
             into oracle/_ref) on a bounded sample of the same workload:
             sampled validation rows x all 65,536 training rows x all 60
             candidates of the first step, one process per host core.
@@ -160,7 +160,7 @@ def _ref_worker_run(rows):
     """Holdout scoring of validation rows ``rows`` with the reference's own
     get_k_nearest_neighbors_cpu: the rows are placed in front of the training
     block as fold 0 (num_per_fold = len(rows)), so each scans exactly the
-    training points; then the kNN mean and squared error as cpu.c:140-150."""
+    training points; then the kNN mean and squared error as cpu.c:56-66."""
     ct = _W["ct"]
     L = _W["lib"]
     Xv, yv, Xt, yt, k = _W["Xv"], _W["yv"], _W["Xt"], _W["yt"], _W["k"]

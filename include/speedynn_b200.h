@@ -137,7 +137,7 @@ SNN_API int snn_step(snn_handle *h);
 /* Warm start / resume: restart from step 0 and commit seq[0..n) in order
  * (forward: features added; backward: features removed) without scoring
  * them, as the reference's distance update would have (the counterpart of
- * compute_distance_matrix_selected, speedynn/lib/cpu.c:269-299 with
+ * compute_distance_matrix_selected, speedynn/lib/cpu.c:185-215 with
  * selected_only, but in commit order so later steps stay bit-identical).
  * Their ordering slots are filled, their errors and best k stay 0.
  * Subsequent snn_step calls continue from step n. */

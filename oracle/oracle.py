@@ -140,7 +140,7 @@ def rmse32(sq):
 # Independent NumPy restatement (tiny inputs only), used to cross-check the C
 # oracle.  Same rules, written vector-wise: neighbour lists are a stable sort
 # of (distance, index) restricted to distance < FLT_MAX, padded with
-# (FLT_MAX, 0) (speedynn/lib/cpu.c:212-252).
+# (FLT_MAX, 0) (speedynn/lib/cpu.c:128-168).
 # --------------------------------------------------------------------------
 def np_loss(labels, preds, lid):
     """speedynn/lib/loss_functions.c:6-183 with the reference's float/double

@@ -35,7 +35,7 @@ def load():
     global _lib
     if _lib is None:
         if not available():
-            raise FileNotFoundError(f"{REF_SO} is not built (make -C oracle with the reference present)")
+            raise FileNotFoundError(f"{REF_SO} is not built (make -C oracle REF=<speedynn checkout>)")
         lib = ctypes.CDLL(REF_SO)
         for name in ("train_forward_selection", "train_backward_selection"):
             fn = getattr(lib, name)
@@ -96,8 +96,8 @@ def loss(labels, preds, loss_function):
 
 def neighbours(X, k_max, k_fold, committed, backward, candidates):
     """Neighbour lists from the reference's own get_k_nearest_neighbors_cpu
-    (speedynn/lib/cpu.c:212-252) after committing ``committed`` into its
-    distance matrix with update_current_dist_matrix_cpu (cpu.c:301-315).
+    (speedynn/lib/cpu.c:128-168) after committing ``committed`` into its
+    distance matrix with update_current_dist_matrix_cpu (cpu.c:217-231).
 
     Returns (idx, dist) of shape [len(candidates), n, k_max].
     """

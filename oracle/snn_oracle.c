@@ -16,23 +16,23 @@
  *
  * What it restates (reference file:line, paths inside the speedynn project):
  *   - fold rule: num_per_fold = n / k_fold, fold(i) = i / num_per_fold
- *     (speedynn/lib/cpu.c:122,132,223); an n % k_fold remainder forms an extra
+ *     (speedynn/lib/cpu.c:38,48,139); an n % k_fold remainder forms an extra
  *     partial fold.
  *   - candidate distance d = D[r,i] + mult*((x_r,c - x_i,c)*(x_r,c - x_i,c)),
- *     product and sum rounded separately (cpu.c:226-228, util.c:19-21).
+ *     product and sum rounded separately (cpu.c:142-144, util.c:19-21).
  *   - top-k_max insertion: slots start at (FLT_MAX, index 0); an item enters
  *     only if strictly below the last slot and bubbles while strictly smaller
- *     (cpu.c:212-252) -> a stable sort by (distance, index) of the items
+ *     (cpu.c:128-168) -> a stable sort by (distance, index) of the items
  *     with distance < FLT_MAX, padded with (FLT_MAX, 0).
  *   - prediction: FP32 sum of labels in neighbour-rank order, then / k
- *     (cpu.c:140-150).
+ *     (cpu.c:56-66).
  *   - RMSE: FP32 sequential sum of squared residuals, / n, sqrt in double,
  *     stored as float (loss_functions.c:41-50).
- *   - best k: first strict minimum in k_vals order (cpu.c:194-204).
+ *   - best k: first strict minimum in k_vals order (cpu.c:111-120).
  *   - best candidate: first strict minimum in ascending dimension order
  *     (nearest_neighbors_feature_selection.c:155-167, :318-329).
  *   - committed distance: forward D = ((0 + s_w0) + s_w1) + ... in selection
- *     order (cpu.c:255-267, :301-315); backward D = sum over all dims taken
+ *     order (cpu.c:171-183, :217-231); backward D = sum over all dims taken
  *     in DESCENDING order (util.c:10-17), then minus each removed dim in
  *     removal order.
  *   - output indexing, auto_feature stop rule, return value

@@ -6,8 +6,10 @@ by the CUDA library through :mod:`speedynn_b200.selector`.  Additions:
 optional ``Xval``/``Yval`` (train on X/Y, score on the validation split
 instead of k-fold CV) and ``device``.  Differences: errors raise exceptions
 instead of ``sys.exit(0)``; ``use_gpu`` is accepted for compatibility, but
-there is no CPU path (the library always runs on the GPU); only kNN
-regression scored by RMSE is on this path.
+there is no CPU path (the library always runs on the GPU).  Every reference
+loss (``loss_functions``, the first one decides) and both model types
+(``"regression"``: kNN mean, ``"classification"``: the reference's mode rule)
+are supported.
 """
 import logging
 

@@ -2,17 +2,17 @@
 //
 // Arithmetic contract (bit parity with speedynn's CPU path):
 //   candidate distance  d = D[r,i] +/- fl(fl(x_r,c - x_i,c)^2)
-//                       (speedynn/lib/cpu.c:226-228, util.c:19-21), every op
+//                       (speedynn/lib/cpu.c:142-144, util.c:19-21), every op
 //                       rounded separately: __fsub_rn/__fmul_rn/__fadd_rn keep
 //                       the compiler from contracting into FMA;
 //   neighbour list      stable (distance, index) order of the items with
 //                       distance < FLT_MAX, padded with (FLT_MAX, 0)
-//                       (cpu.c:212-252);
-//   prediction          FP32 label sum in rank order, then / k (cpu.c:140-150);
+//                       (cpu.c:128-168);
+//   prediction          FP32 label sum in rank order, then / k (cpu.c:56-66);
 //   RMSE                FP32 sequential sum over rows, / n, sqrt in double,
 //                       rounded to float (loss_functions.c:41-50);
 //   committed distance  forward fl(D + s_w) in selection order
-//                       (cpu.c:301-315); backward: full distance summed over
+//                       (cpu.c:217-231); backward: full distance summed over
 //                       dims in descending order (util.c:10-17), then
 //                       fl(D - s_w) in removal order.
 #include <float.h>
@@ -51,8 +51,8 @@ __global__ void k_transpose(const float *__restrict__ X, int n, int p, float *__
 
 // ---------------------------------------------------------------------------
 // Forward start: D = 0 on scored pairs, +inf on excluded / pad columns
-// (speedynn/lib/cpu.c:255-267 zero-fills; exclusion is the fold rule of
-// cpu.c:223 folded into the matrix so the scoring loop needs no test).
+// (speedynn/lib/cpu.c:171-183 zero-fills; exclusion is the fold rule of
+// cpu.c:139 folded into the matrix so the scoring loop needs no test).
 // ---------------------------------------------------------------------------
 __global__ void k_init_forward(Bufs b, int cv, int npf)
 {
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kReduceWarps * 32) k_reduce(Bufs b, int n_cand
 }
 
 // ---------------------------------------------------------------------------
-// Best k per candidate (first strict minimum in k_vals order, cpu.c:194-204),
+// Best k per candidate (first strict minimum in k_vals order, cpu.c:111-120),
 // best candidate (first strict minimum in ascending feature order,
 // nearest_neighbors_feature_selection.c:155-167 / :318-329), bookkeeping as in
 // :169-181 / :331-342, next candidate list, auto stop (:446-465).

@@ -2,10 +2,10 @@
 //
 // For every scored row r and candidate feature c it computes the exact
 // top-k_max neighbour list of
-//     d_i = fl(D[r,i] +/- fl(fl(x_r,c - x_i,c)^2))       (speedynn/lib/cpu.c:226-228)
+//     d_i = fl(D[r,i] +/- fl(fl(x_r,c - x_i,c)^2))       (speedynn/lib/cpu.c:142-144)
 // over all training columns i, in the reference's stable (distance, index)
-// order with (FLT_MAX, 0) padding (cpu.c:212-252), then the kNN-mean
-// prediction for every k of k_vals (cpu.c:140-150).
+// order with (FLT_MAX, 0) padding (cpu.c:128-168), then the kNN-mean
+// prediction for every k of k_vals (cpu.c:56-66).
 //
 // Mapping (B200, 148 SMs, 227 KB shared memory per block):
 //   * a block owns 32 scored rows (lane = row) and W*CC candidates

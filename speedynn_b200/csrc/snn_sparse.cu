@@ -15,7 +15,7 @@
 //     (d < x  <=>  d <= nextafter(x, -inf));
 //   * every member of the true top-k has d <= true k-th <= T_c, so it passes.
 //
-// k_commit_seeds: D <- fl(D +/- s_w) in place (speedynn/lib/cpu.c:301-315),
+// k_commit_seeds: D <- fl(D +/- s_w) in place (speedynn/lib/cpu.c:217-231),
 //   plus, per row, the M smallest new distances (warp per row, list spread
 //   over lanes in registers, cooperative insertion).  HBM-bound.
 // k_score_sparse: warp per row; D streamed once (float4, coalesced); columns

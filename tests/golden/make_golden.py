@@ -11,8 +11,8 @@ inputs + outputs as ``tests/golden/<case>.npz``.  Needs the reference sources
 Each case stores: X, y, method, k_vals, num_features, k_fold, auto_feature and
 the reference outputs ordering, mask, errors (loss 0), best_k, num_final.
 Neighbour cases additionally store the lists returned by the reference's
-get_k_nearest_neighbors_cpu (speedynn/lib/cpu.c:212-252) after committing
-``committed`` with update_current_dist_matrix_cpu (cpu.c:301-315).  Model
+get_k_nearest_neighbors_cpu (speedynn/lib/cpu.c:128-168) after committing
+``committed`` with update_current_dist_matrix_cpu (cpu.c:217-231).  Model
 cases (``model_*``) run the reference with a list of loss ids (the first
 decides) and the regression or classification model, and store every loss of
 every step (``errors_all``, the reference's [loss][p] layout).
