@@ -77,11 +77,9 @@ def job_value(evals_per_rank, ms_max, world):
 
 
 def scoring_kernel(kmax, option=0):
-    """Name of the full-scan scoring kernel the library picks (option 0 = automatic)."""
+    """Name of the scoring kernel the library picks (option 0 = automatic)."""
     if option == 3 or (option == 0 and kmax <= 64):
         return "k_score_tma"
-    if option == 2:
-        return "k_score_rw"
     return "k_score"
 
 
@@ -319,8 +317,9 @@ def run_ours(args, world, rank, local):
     sel = Selector(split.Xtrain, split.ytrain, split.Xval, split.yval, k_vals=[k],
                    num_features=select if backward else steps, method="backward" if backward else "forward",
                    device=local)
-    sel.set_pruning(args.prune)
     sel.set_kernel(args.kernel)
+    if args.seed_step is not None:
+        sel.set_seed_step(args.seed_step)
     for _ in range(args.warmup):
         sel.run()
 
@@ -531,8 +530,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiler captures)")
     ap.add_argument("--no-plain", action="store_true",
                     help="batch workload: skip running the problems one at a time for comparison")
-    ap.add_argument("--prune", type=int, default=0, help="exact pruning of forward steps (library option)")
-    ap.add_argument("--kernel", type=int, default=0, help="full-scan kernel: 0 auto, 1 rows per lane, 2 row tiles per warp, 3 TMA-fed row tiles")
+    ap.add_argument("--kernel", type=int, default=0, help="scoring kernel: 0 auto, 1 rows per lane, 3 TMA-fed row tiles")
+    ap.add_argument("--seed-step", type=int, default=None,
+                    help="first forward step scored from seed bounds (library option; default: the library's)")
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=["fwd-64k", "bwd-50k", "fwd-200k", "batch-64x5"],
                     help="fwd-64k (the headline), bwd-50k (backward, p=120 -> 20), fwd-200k (80 GB distance matrix, "

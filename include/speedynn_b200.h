@@ -175,6 +175,18 @@ SNN_API int snn_get_errors_all(snn_handle *h, float *errors, int n);
 SNN_API int snn_keep_neighbours(snn_handle *h, int enable);
 SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_max, int *idx, float *dist);
 
+/* The kept lists of selected scored rows only (for problems whose full
+ * lists are too large to copy): idx/dist[n_cand][n_sel][k_max] for
+ * rows[0..n_sel), candidates as snn_get_neighbours lists them. */
+SNN_API int snn_get_neighbours_rows(snn_handle *h, const int *rows, int n_sel, int *idx, float *dist);
+
+/* Predictions of the most recent scored step for selected scored rows:
+ * pred[n_cand][num_k_vals][n_sel] (kNN mean, or the mode for
+ * classification), candidates in the order written to cands[n_cand]
+ * (optional; n_cand receives the count).  Available until the next step or
+ * reset, without snn_keep_neighbours. */
+SNN_API int snn_get_predictions(snn_handle *h, const int *rows, int n_sel, int *cands, int *n_cand, float *pred);
+
 /* Kernel time of the last snn_run/snn_step calls (CUDA events on the handle's
  * stream): total milliseconds and launches of the candidate-scoring kernel,
  * of the commit kernel and of everything the selection launched. */
@@ -182,26 +194,23 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
                            int *commit_launches, double *total_ms, int *total_launches);
 
 /* Options:
- *   SNN_OPT_PRUNE  1: forward steps after the first skip training columns
- *                  whose committed distance already exceeds every candidate's
- *                  bound on its k-th neighbour distance (exact: same results;
- *                  pays off only when few columns survive).  Default 0. */
-#define SNN_OPT_PRUNE 1
-/*   SNN_OPT_KERNEL scoring kernel for full scans: 0 automatic (3 for
- *                  k_max <= 64, else 1), 1 rows per lane (any k_max <= 256),
- *                  2 row tiles per warp (k_max <= 64), 3 row tiles fed by a
- *                  TMA/mbarrier ring (k_max <= 64).
- *                  Results are identical; this exists for cross-checks and
- *                  measurement. */
+ *   SNN_OPT_KERNEL scoring kernel: 0 automatic (3 for k_max <= 64, else 1),
+ *                  1 rows per lane (any k_max <= 256), 3 row tiles fed by a
+ *                  TMA/mbarrier ring (k_max <= 64).  Results are identical;
+ *                  this exists for cross-checks and measurement. */
 #define SNN_OPT_KERNEL 2
 /*   SNN_OPT_COUNTERS 1: the TMA-fed scorer keeps the filter counters read by
  *                  snn_get_filter_counters (a little slower).  Default 0. */
 #define SNN_OPT_COUNTERS 3
+/*   SNN_OPT_SEED_STEP forward step (= features already committed) from which
+ *                  the TMA-fed scorer takes each candidate's starting bound on
+ *                  its k-th neighbour distance from 128 "seed" columns near
+ *                  the row (kept by the previous commit) instead of a first
+ *                  pass over a quarter of the columns.  Results are identical;
+ *                  only the work differs.  Default 4; a large value turns it
+ *                  off. */
+#define SNN_OPT_SEED_STEP 4
 SNN_API int snn_set_option(snn_handle *h, int option, int value);
-
-/* Work counters since the last run/step/reset: (row, column) pairs the pruned
- * scorer streamed, and how many of them it had to score. */
-SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, unsigned long long *pairs_survived);
 
 /* Tracing of the TMA-fed scorer since the last run/step/reset: (row, chunk)
  * pairs of its full passes (a chunk = 64 training columns), how many the

@@ -20,9 +20,9 @@ SNN_ERR_NO_WINNER = -5
 SNN_ERR_STATE = -6
 SNN_ERR_TIMEOUT = -7
 
-SNN_OPT_PRUNE = 1
 SNN_OPT_KERNEL = 2
 SNN_OPT_COUNTERS = 3
+SNN_OPT_SEED_STEP = 4
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -74,7 +74,8 @@ def lib():
             "snn_get_timing": (ctypes.c_int, [vp, _f64p, _i32p, _f64p, _i32p, _f64p, _i32p]),
             "snn_destroy": (ctypes.c_int, [vp]),
             "snn_set_option": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
-            "snn_get_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]),
+            "snn_get_neighbours_rows": (ctypes.c_int, [vp, _i32p, ctypes.c_int, _i32p, _f32p]),
+            "snn_get_predictions": (ctypes.c_int, [vp, _i32p, ctypes.c_int, _i32p, _i32p, _f32p]),
             "snn_set_model": (ctypes.c_int, [vp, _i32p, ctypes.c_int, ctypes.c_int]),
             "snn_get_errors_all": (ctypes.c_int, [vp, _f32p, ctypes.c_int]),
             "snn_get_filter_counters": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_ulonglong),

@@ -92,21 +92,21 @@ struct snn_handle {
     int inject_launch = -1;        // fault injection: greedy step whose launch fails once
     bool extra_losses() const { return !(loss_ids.size() == 1 && loss_ids[0] == 0); }
     State *st = nullptr;
-    // pruned forward path
-    float *Xrow = nullptr;        // training points, row-major
-    int *seeds = nullptr;         // [n_rows][M]
-    int M = 0;
-    unsigned long long *survivors = nullptr;
+    // forward: seed columns of each row under the committed D (written by the
+    // commit before a seeded step) and their distances, [n_rows][kSeeds]
+    int *seeds = nullptr;
+    float *seed_d = nullptr;
+    bool seeds_ok = false;        // seeds hold the current D's seed columns
+    int seed_step = 4;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds
     unsigned long long *fcount = nullptr;  // filter counters of the TMA-fed scorer (3)
     bool count_filter = false;             // SNN_OPT_COUNTERS
-    bool prune = false;           // measured slower than the full scan on dense data; opt in
-    int kernel = 0;               // scoring kernel: 0 auto, 1 rows-per-lane, 2 row-per-warp
+    int kernel = 0;               // scoring kernel: 0 auto, 1 rows per lane, 3 TMA-fed row tiles
     int max_smem = 0;
-    unsigned long long scanned_pairs = 0;  // host count of (row, column) pairs the pruned path streamed
     int *nn_idx = nullptr;
     float *nn_dist = nullptr;
     bool keep_nn = false;
     int nn_ncand = 0;
+    int last_ncand = 0;  // candidates of the most recent scored step (prediction slots)
     bool loaded = false;
     int host_step = 0;  // steps issued since the last reset
     // timing
@@ -154,6 +154,9 @@ struct snn_handle {
         b.dmax = dmax;
         b.inject_stall = 0;
         b.fcount = count_filter ? fcount : nullptr;
+        b.seeds = seeds;
+        b.seed_d = seed_d;
+        b.use_seeds = 0;
         return b;
     }
 };
@@ -188,7 +191,7 @@ void free_all(snn_handle *h)
     cudaSetDevice(h->device);
     void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                     h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->Xrow, h->seeds, h->survivors, h->perm, h->fvar,
+                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->perm, h->fvar,
                     h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -228,17 +231,20 @@ int check_device(int device)
     return SNN_OK;
 }
 
-// The pruned scorer needs the seed columns written by the previous forward
-// commit, a k small enough for them, and shared memory for the lists.
-bool use_sparse(const snn_handle *h, int t, int n_cand)
-{
-    if (h->model == 1) return false;  // classification needs every list in full
-    return h->prune && !h->desc.backward && t >= 1 && h->M > 0 && n_cand <= 128 &&
-           snn::sparse_smem_per_warp(n_cand, h->kmax) <= (size_t)h->max_smem;
-}
+// The TMA-fed scorer (k_max <= 64) is the automatic choice; option 1 forces
+// the rows-per-lane scorer (any k_max <= 256).
+bool use_tma(const snn_handle *h) { return h->kernel == 3 || (h->kernel == 0 && snn::score_tma_supported(h->kmax)); }
 
-// Seed columns are only needed by the pruned forward scorer.
-bool seeds_wanted(const snn_handle *h) { return h->prune && !h->desc.backward && h->M > 0; }
+// Forward step t (t features committed) is scored from seed bounds once
+// t >= seed_step: after a few commits the columns nearest under D are near
+// under D + one more feature too, and the seed bound beats a first pass over a
+// quarter of the columns (measured on the fwd-64k data: ~13 list entries per
+// problem against ~47 at step 14, about the same at step 4).  The commit
+// before such a step writes the seeds.
+bool seeds_for_step(const snn_handle *h, int t)
+{
+    return !h->desc.backward && h->seeds && use_tma(h) && t >= h->seed_step;
+}
 
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)
@@ -256,19 +262,14 @@ int issue_step(snn_handle *h, int t)
         return fail(SNN_ERR_CUDA, "injected launch failure at step %d", t);
     }
     bool tma_step = false;
-    if (use_sparse(h, t, n_cand)) {
-        snn::SparseBufs sp{h->Xrow, h->p, h->seeds, h->survivors};
-        SNN_CUDA(snn::launch_score_sparse(b, sp, n_cand, h->M, h->max_smem, h->stream));
-        h->scanned_pairs += (unsigned long long)h->n_rows * h->ldc;
-    } else if (h->kernel == 3 || (h->kernel == 0 && snn::score_tma_supported(h->kmax))) {
+    if (use_tma(h)) {
         b.use_prev = backward && h->prev_ok ? 1 : 0;
+        b.use_seeds = seeds_for_step(h, t) && h->seeds_ok ? 1 : 0;
         b.inject_stall = h->inject_stall + 1;  // 0: off
         h->inject_stall = -1;
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
         h->prev_ok = backward && h->kth_prev;  // this step wrote every candidate's k-th distances
         tma_step = true;
-    } else if (h->kernel != 1 && snn::score_rw_supported(h->kmax)) {
-        SNN_CUDA(snn::launch_score_rw(b, n_cand, backward, h->stream));
     } else {
         SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
     }
@@ -287,12 +288,15 @@ int issue_step(snn_handle *h, int t)
     SNN_CUDA(snn::launch_select(b, n_cand, it, t, h->total_steps, backward, h->desc.auto_feature, h->stream));
     h->n_launch += 3;
     if (h->keep_nn) h->nn_ncand = n_cand;
+    h->last_ncand = n_cand;
     if (t + 1 < h->total_steps) {
         if ((int)h->commit_ev.size() <= h->n_commit) h->commit_ev.resize(h->n_commit + 1);
         EventPair &ce = h->commit_ev[h->n_commit];
         if (int rc = make_pair(ce)) return rc;
         SNN_CUDA(cudaEventRecord(ce.a, h->stream));
-        SNN_CUDA(snn::launch_commit_seeds(b, backward, seeds_wanted(h) ? h->seeds : nullptr, h->M, h->stream));
+        const bool sd = seeds_for_step(h, t + 1);
+        SNN_CUDA(snn::launch_commit(b, backward, sd ? h->seeds : nullptr, sd ? h->seed_d : nullptr, h->stream));
+        h->seeds_ok = sd;
         SNN_CUDA(cudaEventRecord(ce.b, h->stream));
         h->n_commit++;
         h->n_launch += 1;
@@ -303,6 +307,8 @@ int issue_step(snn_handle *h, int t)
 int issue_reset(snn_handle *h)
 {
     h->prev_ok = false;
+    h->seeds_ok = false;
+    h->last_ncand = 0;
     const Bufs b = h->bufs();
     SNN_CUDA(snn::launch_reset_state(b, h->desc.backward, h->total_steps, h->stream));
     if (h->desc.backward) {
@@ -327,8 +333,6 @@ int read_state(snn_handle *h, State *s)
 void reset_timing(snn_handle *h)
 {
     h->n_score = h->n_commit = h->n_launch = 0;
-    h->scanned_pairs = 0;
-    if (h->survivors) cudaMemsetAsync(h->survivors, 0, sizeof(unsigned long long), h->stream);
     if (h->fcount) cudaMemsetAsync(h->fcount, 0, 3 * sizeof(unsigned long long), h->stream);
 }
 
@@ -373,8 +377,9 @@ static size_t handle_bytes(const snn_desc *d, int kmax)
     const size_t n_rows = cv ? n_cols : (size_t)d->n_val;
     const size_t ldc = (size_t)round_up(d->n_train, snn::kPadCols);
     const size_t ldr = cv ? ldc : (size_t)round_up((int)n_rows, snn::kPadCols);
-    const size_t M = d->backward ? 0 : (size_t)snn::seeds_for_k(kmax);
-    size_t f = p * ldc + n_rows * ldc + p * (size_t)d->num_k_vals * n_rows + p * n_cols + std::max(n_rows, n_cols) * p +
+    const size_t M = d->backward ? 0 : 2 * (size_t)snn::kSeeds;  // seed columns and distances
+    (void)kmax;
+    size_t f = p * ldc + n_rows * ldc + p * (size_t)d->num_k_vals * n_rows + std::max(n_rows, n_cols) * p +
                n_rows * M + n_cols + n_rows;
     if (d->backward) f += p * n_rows + n_rows;  // kth_prev, dmax
     if (!cv) f += p * ldr;
@@ -459,11 +464,11 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if ((rc = dev_alloc(&h->order, p, "ordering"))) return bail(rc);
     if ((rc = dev_alloc(&h->stepk, p, "best k"))) return bail(rc);
     if ((rc = dev_alloc(&h->st, 1, "state"))) return bail(rc);
-    if ((rc = dev_alloc(&h->Xrow, p * h->n_cols, "X_train rows"))) return bail(rc);
-    if ((rc = dev_alloc(&h->survivors, 1, "counters"))) return bail(rc);
     if ((rc = dev_alloc(&h->fcount, 3, "filter counters"))) return bail(rc);
-    h->M = d->backward ? 0 : snn::seeds_for_k(kmax);
-    if (h->M > 0 && (rc = dev_alloc(&h->seeds, (size_t)h->n_rows * h->M, "seed columns"))) return bail(rc);
+    if (!d->backward) {
+        if ((rc = dev_alloc(&h->seeds, (size_t)h->n_rows * snn::kSeeds, "seed columns"))) return bail(rc);
+        if ((rc = dev_alloc(&h->seed_d, (size_t)h->n_rows * snn::kSeeds, "seed distances"))) return bail(rc);
+    }
     // On the handle's stream, so every kernel that reads k_vals comes after it
     // (the source lives as long as the handle).  A cudaMemcpy here would run on
     // the legacy stream, which does not order the handle's non-blocking stream,
@@ -502,8 +507,6 @@ static int load_impl(snn_handle *h, const float *X_train, const float *y_train, 
     SNN_CUDA(cudaSetDevice(h->device));
     const cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (int rc = load_matrix(h, X_train, h->n_cols, h->XT, h->ldc, device_src)) return rc;
-    SNN_CUDA(cudaMemcpyAsync(h->Xrow, device_src ? X_train : h->stage, sizeof(float) * (size_t)h->n_cols * h->p,
-                             cudaMemcpyDeviceToDevice, h->stream));
     SNN_CUDA(cudaMemcpyAsync(h->yc, y_train, sizeof(float) * h->n_cols, kind, h->stream));
     if (!h->cv) {
         // the staging buffer is reused: order the second upload after the first transpose
@@ -611,7 +614,9 @@ SNN_API int snn_commit_sequence(snn_handle *h, const int *seq, int n)
     for (int t = 0; t < n; ++t) {
         const int it = h->desc.backward ? h->p - 1 - t : t;
         SNN_CUDA(snn::launch_force(b, seq[t], it, t, h->total_steps, h->desc.backward, h->stream));
-        SNN_CUDA(snn::launch_commit_seeds(b, h->desc.backward, seeds_wanted(h) ? h->seeds : nullptr, h->M, h->stream));
+        const bool sd = t + 1 == n && seeds_for_step(h, n);  // the step after the sequence may use seeds
+        SNN_CUDA(snn::launch_commit(b, h->desc.backward, sd ? h->seeds : nullptr, sd ? h->seed_d : nullptr, h->stream));
+        h->seeds_ok = sd;
     }
     h->host_step = n;
     SNN_CUDA(cudaStreamSynchronize(h->stream));
@@ -723,6 +728,75 @@ SNN_API int snn_get_neighbours(snn_handle *h, int *cands, int *n_cand, int *k_ma
     return SNN_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Copy the rows rows[0..n_sel) of a [n_cand][n_rows][w] device array into
+// out[n_cand][n_sel][w], one candidate slab at a time through a host buffer.
+template <typename T>
+int gather_rows(snn_handle *h, const T *dev, int n_cand, int w, const int *rows, int n_sel, T *out)
+{
+    std::vector<T> slab((size_t)h->n_rows * w);
+    for (int c = 0; c < n_cand; ++c) {
+        SNN_CUDA(cudaMemcpyAsync(slab.data(), dev + (size_t)c * h->n_rows * w, sizeof(T) * slab.size(),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        SNN_CUDA(cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < n_sel; ++i)
+            memcpy(out + ((size_t)c * n_sel + i) * w, slab.data() + (size_t)rows[i] * w, sizeof(T) * w);
+    }
+    return SNN_OK;
+}
+
+int check_rows(const snn_handle *h, const int *rows, int n_sel)
+{
+    if (n_sel < 0 || (n_sel > 0 && !rows)) return fail(SNN_ERR_ARG, "rows must list n_sel >= 0 row indices");
+    for (int i = 0; i < n_sel; ++i)
+        if (rows[i] < 0 || rows[i] >= h->n_rows)
+            return fail(SNN_ERR_ARG, "row %d (=%d) outside [0, %d)", i, rows[i], h->n_rows);
+    return SNN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+SNN_API int snn_get_neighbours_rows(snn_handle *h, const int *rows, int n_sel, int *idx, float *dist)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (!h->keep_nn || h->nn_ncand == 0) return fail(SNN_ERR_STATE, "no neighbour lists kept (snn_keep_neighbours)");
+    if (int rc = check_rows(h, rows, n_sel)) return rc;
+    SNN_CUDA(cudaSetDevice(h->device));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    if (idx) {
+        if (int rc = gather_rows(h, h->nn_idx, h->nn_ncand, h->kmax, rows, n_sel, idx)) return rc;
+    }
+    if (dist) {
+        if (int rc = gather_rows(h, h->nn_dist, h->nn_ncand, h->kmax, rows, n_sel, dist)) return rc;
+    }
+    return SNN_OK;
+}
+
+SNN_API int snn_get_predictions(snn_handle *h, const int *rows, int n_sel, int *cands, int *n_cand, float *pred)
+{
+    g_err.clear();
+    if (!h) return fail(SNN_ERR_ARG, "null handle");
+    if (h->last_ncand == 0) return fail(SNN_ERR_STATE, "no step has been scored since the last reset");
+    if (int rc = check_rows(h, rows, n_sel)) return rc;
+    SNN_CUDA(cudaSetDevice(h->device));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    if (n_cand) *n_cand = h->last_ncand;
+    if (cands)
+        SNN_CUDA(cudaMemcpyAsync(cands, h->prev_cands, sizeof(int) * h->last_ncand, cudaMemcpyDeviceToHost, h->stream));
+    if (pred) {
+        // pred is [slot][k][n_rows]: gather as [slot * nk + m] slabs of n_rows values
+        if (int rc = gather_rows(h, h->pred, h->last_ncand * h->nk, 1, rows, n_sel, pred)) return rc;
+    }
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    return SNN_OK;
+}
+
 SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches, double *commit_ms, int *commit_launches,
                            double *total_ms, int *total_launches)
 {
@@ -763,31 +837,21 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value)
     g_err.clear();
     if (!h) return fail(SNN_ERR_ARG, "null handle");
     switch (option) {
-    case SNN_OPT_PRUNE: h->prune = value != 0; return SNN_OK;
     case SNN_OPT_KERNEL:
-        if (value < 0 || value > 3) return fail(SNN_ERR_ARG, "kernel choice %d not in 0..3", value);
-        if (value == 2 && !snn::score_rw_supported(h->kmax))
-            return fail(SNN_ERR_UNSUPPORTED, "the row-tile kernel handles k_max <= 64");
+        if (value != 0 && value != 1 && value != 3) return fail(SNN_ERR_ARG, "kernel choice %d is not 0, 1 or 3", value);
         if (value == 3 && !snn::score_tma_supported(h->kmax))
             return fail(SNN_ERR_UNSUPPORTED, "the TMA-fed kernel handles k_max <= 64");
         h->kernel = value;
+        h->seeds_ok = false;
+        return SNN_OK;
+    case SNN_OPT_SEED_STEP:
+        if (value < 1) return fail(SNN_ERR_ARG, "seed step %d must be >= 1", value);
+        h->seed_step = value;
+        h->seeds_ok = false;
         return SNN_OK;
     case SNN_OPT_COUNTERS: h->count_filter = value != 0; return SNN_OK;
     default: return fail(SNN_ERR_ARG, "unknown option %d", option);
     }
-}
-
-SNN_API int snn_get_counters(snn_handle *h, unsigned long long *pairs_streamed, unsigned long long *pairs_survived)
-{
-    g_err.clear();
-    if (!h) return fail(SNN_ERR_ARG, "null handle");
-    SNN_CUDA(cudaSetDevice(h->device));
-    unsigned long long sv = 0;
-    SNN_CUDA(cudaMemcpyAsync(&sv, h->survivors, sizeof sv, cudaMemcpyDeviceToHost, h->stream));
-    SNN_CUDA(cudaStreamSynchronize(h->stream));
-    if (pairs_streamed) *pairs_streamed = h->scanned_pairs;
-    if (pairs_survived) *pairs_survived = sv;
-    return SNN_OK;
 }
 
 SNN_API int snn_get_filter_counters(snn_handle *h, unsigned long long *row_chunks, unsigned long long *flagged,

@@ -1,0 +1,151 @@
+// snn_commit.cu -- commit the winning feature into the distance matrix.
+//
+// k_commit: D <- fl(D +/- fl((x_r,w - x_i,w)^2)) in place for the winner w of
+// the step that just ran (read from the device state, so the host never waits
+// for it): speedynn/lib/cpu.c:217-231 and
+// kernels/update_current_distance_matrix_float.cl:5-32, with the product and
+// the sum rounded separately.  A warp streams one row with 16-byte loads and
+// stores (HBM-bound: 8 bytes per entry).
+//
+// Seeds (forward steps only).  While it streams a row, each lane also keeps
+// the four smallest new distances among the columns it visits (lane l sees
+// the float4 groups l, l+32, l+64, ...), so every row leaves 128 distinct
+// real columns that lie near it under the committed features: seeds[r][j*32+l]
+// and their distances seed_d[r][j*32+l] (lane l's j-th smallest; index -1 and
+// +inf where a lane saw fewer than four finite distances).  The next forward
+// scoring launch takes, for each candidate, the k-th smallest exact distance
+// over these columns as its starting bound on the candidate's k-th neighbour
+// distance (any k distinct columns bound it; near ones bound it tightly), in
+// place of a first pass over the columns.
+#include <float.h>
+#include <math.h>
+
+#include "snn_internal.h"
+
+namespace snn {
+
+namespace {
+
+__device__ __forceinline__ float sqdiff(float a, float b)
+{
+    const float t = __fsub_rn(a, b);
+    return __fmul_rn(t, t);
+}
+
+// Insert (v, col) into the lane's ascending four-entry list if v is below its
+// last entry (strict: +inf and NaN never enter).
+__device__ __forceinline__ void keep4(float (&s)[4], int (&i)[4], float v, int col)
+{
+    if (!(v < s[3])) return;
+    if (v < s[2]) {
+        s[3] = s[2];
+        i[3] = i[2];
+        if (v < s[1]) {
+            s[2] = s[1];
+            i[2] = i[1];
+            if (v < s[0]) {
+                s[1] = s[0];
+                i[1] = i[0];
+                s[0] = v;
+                i[0] = col;
+            } else {
+                s[1] = v;
+                i[1] = col;
+            }
+        } else {
+            s[2] = v;
+            i[2] = col;
+        }
+    } else {
+        s[3] = v;
+        i[3] = col;
+    }
+}
+
+template <bool BWD, bool SEEDS>
+__global__ void __launch_bounds__(256) k_commit(Bufs b, int *seeds, float *seed_d)
+{
+    if (b.st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int w = b.st->winner;
+    const float *xt = b.XT + (size_t)w * b.ldc;
+    const float *xv = b.XV + (size_t)w * b.ldr;
+    const float4 *xt4 = reinterpret_cast<const float4 *>(xt);
+    const int n4 = b.ldc >> 2;
+    for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < b.n_rows; r += gridDim.x * wpb) {
+        const float a = __ldg(xv + r);
+        float4 *row = reinterpret_cast<float4 *>(b.D + (size_t)r * b.ldc);
+        float sv[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+        int si[4] = {-1, -1, -1, -1};
+        for (int q0 = 0; q0 < n4; q0 += 128) {  // 4 float4 per lane in flight
+            float4 d[4], c[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + u * 32 + lane;
+                if (q < n4) {
+                    d[u] = __ldcs(row + q);
+                    c[u] = __ldg(xt4 + q);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + u * 32 + lane;
+                if (q < n4) {
+                    if (BWD) {
+                        d[u].x = __fsub_rn(d[u].x, sqdiff(a, c[u].x));
+                        d[u].y = __fsub_rn(d[u].y, sqdiff(a, c[u].y));
+                        d[u].z = __fsub_rn(d[u].z, sqdiff(a, c[u].z));
+                        d[u].w = __fsub_rn(d[u].w, sqdiff(a, c[u].w));
+                    } else {
+                        d[u].x = __fadd_rn(d[u].x, sqdiff(a, c[u].x));
+                        d[u].y = __fadd_rn(d[u].y, sqdiff(a, c[u].y));
+                        d[u].z = __fadd_rn(d[u].z, sqdiff(a, c[u].z));
+                        d[u].w = __fadd_rn(d[u].w, sqdiff(a, c[u].w));
+                    }
+                    __stcs(row + q, d[u]);
+                    if (SEEDS) {
+                        keep4(sv, si, d[u].x, 4 * q);
+                        keep4(sv, si, d[u].y, 4 * q + 1);
+                        keep4(sv, si, d[u].z, 4 * q + 2);
+                        keep4(sv, si, d[u].w, 4 * q + 3);
+                    }
+                }
+            }
+        }
+        if (SEEDS) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                seeds[(size_t)r * kSeeds + j * 32 + lane] = si[j];
+                seed_d[(size_t)r * kSeeds + j * 32 + lane] = sv[j];
+            }
+        }
+    }
+}
+
+int sm_count_commit()
+{
+    // initialised once, thread-safely (handles may be created from several threads)
+    static const int n = [] {
+        int dev = 0, c = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        return c > 0 ? c : 148;
+    }();
+    return n;
+}
+
+}  // namespace
+
+cudaError_t launch_commit(const Bufs &b, int backward, int *seeds, float *seed_d, cudaStream_t s)
+{
+    int grid = (b.n_rows + 7) / 8;
+    const int cap = sm_count_commit() * 8;
+    if (grid > cap) grid = cap;
+    if (backward) k_commit<true, false><<<grid, 256, 0, s>>>(b, nullptr, nullptr);
+    else if (seeds && seed_d) k_commit<false, true><<<grid, 256, 0, s>>>(b, seeds, seed_d);
+    else k_commit<false, false><<<grid, 256, 0, s>>>(b, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+}  // namespace snn

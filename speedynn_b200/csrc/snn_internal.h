@@ -67,6 +67,12 @@ struct Bufs {
     // optional filter counters of the TMA-fed scorer: [0] (row, chunk) pairs of
     // the full pass, [1] of them flagged by the filter, [2] holding an exact pass
     unsigned long long *fcount;
+    // forward: kSeeds columns per row near it under the committed D, and their
+    // distances [n_rows][kSeeds] (written by the previous step's commit); when
+    // use_seeds is set the TMA-fed scorer takes its starting bounds from them
+    const int *seeds;
+    const float *seed_d;
+    int use_seeds;
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D
@@ -91,22 +97,10 @@ void clear_error();
 bool score_tma_supported(int kmax);  // kernel option 3: k_max <= 64
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
 
-// Row-per-warp scoring (snn_score_rw.cu), k_max <= 64.
-bool score_rw_supported(int kmax);
-cudaError_t launch_score_rw(const Bufs &b, int n_cand, int backward, cudaStream_t s);
-
-// Pruned forward scoring (snn_sparse.cu).
-constexpr int kMaxSeeds = 128;  // seed columns per row (multiple of 32)
-struct SparseBufs {
-    const float *Xrow;                  // training points, row-major [n_cols][ldp]
-    int ldp;
-    int *seeds;                         // [n_rows][M] nearest columns under the committed D
-    unsigned long long *survivors;      // optional counter of scanned-in columns
-};
-size_t sparse_smem_per_warp(int n_cand, int kmax);
-int seeds_for_k(int kmax);  // 0: k too large for the pruned path
-cudaError_t launch_commit_seeds(const Bufs &b, int backward, int *seeds, int M, cudaStream_t s);
-cudaError_t launch_score_sparse(const Bufs &b, const SparseBufs &sp, int n_cand, int M, int max_smem, cudaStream_t s);
+// Commit the winner into D (snn_commit.cu); forward commits given seed
+// buffers also keep kSeeds near columns per row for the next step's bounds.
+constexpr int kSeeds = 128;  // seed columns per row: four per lane of a warp
+cudaError_t launch_commit(const Bufs &b, int backward, int *seeds, float *seed_d, cudaStream_t s);
 
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);
 cudaError_t launch_init_forward(const Bufs &b, int cv, int npf, cudaStream_t s);

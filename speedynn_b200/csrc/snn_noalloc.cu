@@ -11,23 +11,28 @@
 // static __device__ array of fixed size.  It calls no cudaMalloc, cudaFree or
 // allocating library routine.
 //
-// The array lives for as long as the library is loaded, on every GPU that
-// runs this code.  All calls share it and it keeps the last call's contents,
-// so calls whose GPU work overlaps (two host threads, or two streams, with
-// work in flight at the same time) race on it; run them one after another.
+// The array is device memory of the library's own module: the CUDA runtime
+// places it on a GPU when it loads this library's kernels there (with lazy
+// loading, the CUDA 12 default, at the first launch or symbol lookup of the
+// library on that GPU -- the first call of this or any other entry point),
+// and it stays there until the process exits.  A caller with a strict
+// no-allocation window should make one call (or any library call) on each GPU
+// before the window opens.  All calls share the array and it keeps the last
+// call's contents, so calls whose GPU work overlaps (two host threads, or two
+// streams, with work in flight at the same time) race on it; run them one
+// after another.
 #include <float.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "../../include/speedynn_b200.h"
 #include "snn_internal.h"
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 constexpr size_t kStateFloats = 64;     // snn::State, padded to 256 bytes
 constexpr size_t kKvFloats = 256;       // k values
 constexpr size_t kCandFloats = 1024;    // candidate feature ids
@@ -40,25 +45,20 @@ static_assert(sizeof(snn::State) <= kStateFloats * sizeof(float), "state must fi
 // is only a stand-in, so the device address is looked up per device below.
 static __device__ __align__(256) float g_step_scratch[kScratchFloats];
 
-std::mutex g_mu;
-float *g_addr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch on the current device (looked up once per device).
-int scratch_address(int dev, float **out)
+// Device address of the scratch on the current device.  Looked up on every
+// call (a cheap runtime query) rather than cached: after a device reset the
+// module is loaded again and the array may sit at another address.
+int scratch_address(float **out)
 {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_step_scratch);
-        if (e != cudaSuccess || !p) {
-            char msg[256];
-            snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the step scratch failed: %s", cudaGetErrorString(e));
-            cudaGetLastError();
-            return snn::record_error(SNN_ERR_CUDA, msg);
-        }
-        g_addr[dev] = static_cast<float *>(p);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_step_scratch);
+    if (e != cudaSuccess || !p) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the step scratch failed: %s", cudaGetErrorString(e));
+        cudaGetLastError();
+        return snn::record_error(SNN_ERR_CUDA, msg);
     }
-    *out = g_addr[dev];
+    *out = static_cast<float *>(p);
     return SNN_OK;
 }
 
@@ -98,18 +98,18 @@ extern "C" SNN_API int snn_score_step_noalloc(const float *D, int ld, const floa
     }
     for (int c = 0; c < n_cand; ++c)
         if (cands[c] < 0 || cands[c] >= p) return err(SNN_ERR_ARG, "snn_score_step_noalloc: candidate id outside [0, p)");
+    if ((reinterpret_cast<uintptr_t>(D) | reinterpret_cast<uintptr_t>(XT)) & 15u)
+        return err(SNN_ERR_ARG, "snn_score_step_noalloc: D and XT must be 16-byte aligned (they are read by TMA copies)");
 
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_err(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices) return err(SNN_ERR_ARG, "snn_score_step_noalloc: device ordinal above 63");
     float *base = nullptr;
-    if (int rc = scratch_address(dev, &base)) return rc;
+    if (int rc = scratch_address(&base)) return rc;
     int max_smem = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const snn::ScorePlan plan = snn::plan_score(kmax, n_cand, max_smem);
-    if (plan.cc == 0 && !snn::score_rw_supported(kmax))
-        return err(SNN_ERR_UNSUPPORTED, "snn_score_step_noalloc: k_max above 256");
+    if (plan.cc == 0) return err(SNN_ERR_UNSUPPORTED, "snn_score_step_noalloc: k_max above 256");
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     snn::State *st = reinterpret_cast<snn::State *>(base);
@@ -146,7 +146,6 @@ extern "C" SNN_API int snn_score_step_noalloc(const float *D, int ld, const floa
     b.st = st;
 
     if (snn::score_tma_supported(kmax)) e = snn::launch_score_tma(b, n_cand, backward, s);
-    else if (snn::score_rw_supported(kmax)) e = snn::launch_score_rw(b, n_cand, backward, s);
     else e = snn::launch_score(b, n_cand, plan, backward, s);
     if (e != cudaSuccess) return cuda_err(e, "scoring kernel launch");
     if ((e = snn::launch_reduce(b, n_cand, s)) != cudaSuccess) return cuda_err(e, "error reduction launch");

@@ -1,8 +1,10 @@
 // snn_score_tma.cu -- candidate scoring, warp-specialised TMA pipeline.
 //
-// Contract as snn_score_rw.cu: exact top-k_max lists (k <= 64) in the
-// reference's stable (distance, index) order and kNN-mean predictions.  A
-// block scores 24 rows x 12 candidates; each of its 18 consumer warps owns 4
+// For every (scored row, candidate): the exact top-k_max list (k <= 64) of
+// d_i = fl(D[r,i] +/- fl((x_r,c - x_i,c)^2)) over the training columns i in
+// the reference's stable (distance, index) order
+// (speedynn/lib/cpu.c:128-168) and the kNN-mean predictions (cpu.c:56-66).
+// A block scores 24 rows x 12 candidates; each of its 18 consumer warps owns 4
 // rows x 4 candidates and walks the columns two per lane with packed f32x2
 // (18 consumers + 1 producer = 19 warps, at most 5 per SM sub-partition at 96
 // registers; 12-candidate groups leave no padded slot for 60 candidates).
@@ -16,10 +18,13 @@
 //     mbarrier; consumers release a slot through its "empty" mbarrier, so a
 //     warp busy inserting falls behind by up to a ring of stages without
 //     stalling the others.
-//   * First pass over a quarter of the columns: per-lane minima; their k-th
-//     smallest bounds the final k-th distance (k distinct columns lie at or
-//     below it).  Backward steps after the first skip it and start from the
-//     previous step's k-th distances (kth_prev), which removal only lowers.
+//   * Starting bound on each problem's k-th distance (k distinct columns lie
+//     at or below it): a first pass over a quarter of the columns (per-lane
+//     minima, their k-th smallest); or, on seeded forward steps, the k-th
+//     smallest exact distance over the row's 128 seed columns (the columns
+//     nearest the row under the committed D, kept by the last commit); or, on
+//     backward steps after the first, the previous step's k-th distances
+//     (kth_prev), which removal only lowers.
 //   * Full pass: a conservative sign-bit filter (one sub and one FMA per
 //     evaluation; filter_bound / filter_bound_bwd) flags rows that may hold a
 //     passing column; flagged rows are re-scored with the reference's
@@ -323,6 +328,78 @@ __device__ __forceinline__ float warp_sort32(float v, int lane)
     return v;
 }
 
+// Ascending bitonic sort of 32*V values over the warp, V per lane: lane l
+// holds elements V*l .. V*l+V-1 (NaN must not occur: fminf/fmaxf would drop it).
+template <int V>
+__device__ __forceinline__ void warp_sort_v(float (&v)[V], int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32 * V; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= V) {  // partner in lane ^ (j / V), same slot
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    const float o = __shfl_xor_sync(kFull, v[h], j / V);
+                    const int i = V * lane + h;
+                    v[h] = (((i & j) == 0) == ((i & k) == 0)) ? fminf(v[h], o) : fmaxf(v[h], o);
+                }
+            } else {  // partner in the same lane
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    if ((h & j) == 0) {
+                        const bool up = ((V * lane + h) & k) == 0;
+                        const float a = v[h], c = v[h + j];
+                        v[h] = up ? fminf(a, c) : fmaxf(a, c);
+                        v[h + j] = up ? fmaxf(a, c) : fminf(a, c);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// K-th smallest (1-based, K <= 32*V) of the 32*V values v[] over the warp.
+template <int V>
+__device__ __forceinline__ float warp_kth(float (&v)[V], int K, int lane)
+{
+    warp_sort_v<V>(v, lane);
+    float sel = v[0];
+#pragma unroll
+    for (int h = 1; h < V; ++h)
+        if (h == (K - 1) % V) sel = v[h];
+    return __shfl_sync(kFull, sel, (K - 1) / V);
+}
+
+// Starting bound of one forward problem from the scored row's kSeeds seed
+// columns (snn_commit.cu): the K-th smallest exact distance
+// d = fl(D + fl((x - x_i)^2)) over them.  Any K distinct columns have their
+// K-th smallest distance at or above the final K-th neighbour distance, so it
+// is an inclusive bound; padding seeds (index -1) and NaN distances count as
+// +inf.  sd[j], si[j]: the row's seeds j*32 + lane; xc: the candidate's
+// training values.  For K <= 32 the K-th of the 64 values made of each lane's
+// two smallest is taken (a subset: still K distinct columns, and as tight as
+// all 128 unless a lane holds three of the K nearest).
+template <int KL>
+__device__ __forceinline__ float seed_bound(const float (&sd)[4], const int (&si)[4], float x, const float *xc, int K,
+                                            int lane)
+{
+    float v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float d = si[j] >= 0 ? __fadd_rn(sd[j], sqdiff1(x, __ldg(xc + si[j]))) : INFINITY;
+        v[j] = d <= FLT_MAX ? d : INFINITY;
+    }
+    if constexpr (KL > 32) {
+        return warp_kth<4>(v, K, lane);
+    } else {
+        const float a = fminf(v[0], v[1]), b = fmaxf(v[0], v[1]);
+        const float c = fminf(v[2], v[3]), e = fmaxf(v[2], v[3]);
+        float two[2] = {fminf(a, c), fminf(fmaxf(a, c), fminf(b, e))};
+        return warp_kth<2>(two, K, lane);
+    }
+}
+
 struct TmaSmem {
     float *Ds, *Xs, *Lds, *thr_s, *xv_s;
     int *Lis, *srcand, *wcnt;
@@ -389,7 +466,10 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int
     // Backward steps after the first reuse the last step's k-th distances as
     // bounds (D only shrinks when a feature is removed) and skip the first pass.
     const bool reuse = BWD && b.use_prev && b.kth_prev != nullptr;
-    const int nA = reuse ? 0 : (nstages >= 4 ? nstages / 4 : 1);
+    // Seeded forward steps take their bounds from the previous commit's seed
+    // columns and skip the first pass as well.
+    const bool seeded = !BWD && b.use_seeds && b.seeds != nullptr && b.seed_d != nullptr;
+    const int nA = reuse || seeded ? 0 : (nstages >= 4 ? nstages / 4 : 1);
     const int nvirt = nA + nstages;
 
     if (w == kConsumers) {
@@ -484,7 +564,32 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int
     // derived from it is widened by 2^-20 relative (see fwd_bound).
     // For k_max > 32 each lane keeps two minima (its even and its odd columns),
     // 64 values from distinct columns.
-    {
+    if (seeded) {
+        // One problem at a time (warp-uniform): gather the candidate's values at
+        // the row's seed columns, exact distances, K-th smallest.
+#pragma unroll 1
+        for (int ri = 0; ri < kRW; ++ri) {
+            const int r = wr0 + ri;
+            float sd[4];
+            int si[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                si[j] = r < b.n_rows ? __ldg(b.seeds + (size_t)r * kSeeds + j * 32 + lane) : -1;
+                sd[j] = r < b.n_rows ? __ldg(b.seed_d + (size_t)r * kSeeds + j * 32 + lane) : INFINITY;
+            }
+#pragma unroll 1
+            for (int ci = 0; ci < kCW; ++ci) {
+                const int p = ri * kCW + ci;
+                float th = -1.0f;  // padded problem: never passes
+                if ((okmask >> p) & 1u) {
+                    const float T = seed_bound<KL>(sd, si, myX[p], b.XT + (size_t)S.srcand[wc + ci] * b.ldc, K, lane);
+                    th = T < FLT_MAX ? T : 0x1.fffffcp+127f;  // inclusive; FLT_MAX itself never enters
+                }
+                if (lane == 0) myT[p] = th;
+            }
+        }
+        __syncwarp();
+    } else {
         float mn[kP], mn2[kP];  // mn2: LONG only
 #pragma unroll
         for (int p = 0; p < kP; ++p) mn[p] = mn2[p] = INFINITY;

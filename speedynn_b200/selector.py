@@ -120,18 +120,38 @@ class Selector:
                                    ptr(dist, _f32p)))
         return cands, idx, dist
 
-    def set_pruning(self, enable):
-        """Exact pruning of forward steps after the first (off by default)."""
-        check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_PRUNE, int(bool(enable))))
+    def neighbours_rows(self, rows):
+        """idx/dist [n_cand, len(rows), k_max] of the last kept step for the given scored rows."""
+        L = _lib.lib()
+        nc = ctypes.c_int()
+        km = ctypes.c_int()
+        check(L.snn_get_neighbours(self._h, None, ctypes.byref(nc), ctypes.byref(km), None, None))
+        r = np.ascontiguousarray(rows, dtype=np.int32).reshape(-1)
+        idx = np.zeros((nc.value, r.size, km.value), np.int32)
+        dist = np.zeros((nc.value, r.size, km.value), np.float32)
+        check(L.snn_get_neighbours_rows(self._h, ptr(r, _i32p), r.size, ptr(idx, _i32p), ptr(dist, _f32p)))
+        return idx, dist
+
+    def predictions(self, rows):
+        """(candidates, pred [n_cand, num_k_vals, len(rows)]) of the most recent scored step."""
+        L = _lib.lib()
+        r = np.ascontiguousarray(rows, dtype=np.int32).reshape(-1)
+        nc = ctypes.c_int()
+        check(L.snn_get_predictions(self._h, ptr(r, _i32p), 0, None, ctypes.byref(nc), None))
+        cands = np.zeros(nc.value, np.int32)
+        pred = np.zeros((nc.value, self.k_vals.size, r.size), np.float32)
+        check(L.snn_get_predictions(self._h, ptr(r, _i32p), r.size, ptr(cands, _i32p), ctypes.byref(nc),
+                                    ptr(pred, _f32p)))
+        return cands, pred
 
     def set_kernel(self, which):
-        """Full-scan scoring kernel: 0 automatic, 1 rows per lane, 2 row per warp."""
+        """Scoring kernel: 0 automatic, 1 rows per lane (any k), 3 TMA-fed row tiles (k <= 64)."""
         check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_KERNEL, int(which)))
 
-    def counters(self):
-        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
-        check(_lib.lib().snn_get_counters(self._h, ctypes.byref(a), ctypes.byref(b)))
-        return {"pairs_streamed": a.value, "pairs_survived": b.value}
+    def set_seed_step(self, step):
+        """First forward step whose starting bounds come from seed columns (default 4;
+        a large value turns seeded steps off).  Results do not depend on it."""
+        check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_SEED_STEP, int(step)))
 
     def set_counters(self, enable):
         """Keep the TMA-fed scorer's filter counters (off by default: a little slower)."""

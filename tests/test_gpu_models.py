@@ -65,14 +65,14 @@ def _classify(y):
     return np.digitize(y, np.quantile(y, [0.33, 0.66])).astype(np.float32)
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("variant", ["lanes", "tma", "tma_seeded"])
 @pytest.mark.parametrize("case", [
     dict(losses=[2, 0, 4, 6], model=0, kv=[3, 8], method="forward", nf=4),
     dict(losses=[1, 5, 8], model=0, kv=[5], method="backward", nf=5),
     dict(losses=[4, 3], model=1, kv=[1, 4, 7], method="forward", nf=4),
     dict(losses=[4], model=1, kv=[2, 6], method="backward", nf=4),
 ])
-def test_holdout_models_match_restatement(case, kernel):
+def test_holdout_models_match_restatement(case, variant):
     s = datagen.generate(320, 110, 9, n_mag=5, seed=90 + len(case["losses"]) + case["model"])
     yt, yv = s.ytrain, s.yval
     if case["model"] == 1:
@@ -82,7 +82,9 @@ def test_holdout_models_match_restatement(case, kernel):
                          model_type=case["model"])
     with Selector(s.Xtrain, yt, s.Xval, yv, k_vals=case["kv"], num_features=case["nf"], method=case["method"],
                   loss_functions=case["losses"], model_type=case["model"]) as sel:
-        sel.set_kernel(kernel)
+        sel.set_kernel(1 if variant == "lanes" else 3)
+        if variant == "tma_seeded":
+            sel.set_seed_step(1)
         r = sel.run()
     np.testing.assert_array_equal(r["ordering"], o["ordering"])
     np.testing.assert_array_equal(r["mask"], o["mask"])

@@ -18,7 +18,10 @@ from speedynn_b200.selector import Selector
 pytestmark = pytest.mark.gpu
 
 GDIR = os.path.join(ROOT, "tests", "golden")
-SELECT_CASES = [n for n in golden_cases() if not n.startswith(("nn_", "model_")) and n != "losses"]
+SELECT_CASES = [n for n in golden_cases() if not n.startswith(("nn_", "model_", "config_")) and n != "losses"]
+# scoring variants: rows-per-lane kernel; TMA-fed kernel with the default seed
+# step; TMA-fed kernel with seeded bounds from the second forward step on
+VARIANTS = ["lanes", "tma", "tma_seeded"]
 NN_CASES = golden_cases("nn_")
 ERR64_RTOL = 1e-9
 
@@ -90,12 +93,27 @@ def test_neighbour_lists_match_reference(name):
         np.testing.assert_array_equal(dist[j], g["nn_dist"][ci])
 
 
-def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, kernel=0, **kw):
+def configure(sel, variant):
+    """Select a scoring variant on a Selector (results must not depend on it)."""
+    if variant == "lanes":
+        sel.set_kernel(1)
+    elif variant in ("tma", "tma_seeded"):
+        sel.set_kernel(3)
+        if variant == "tma_seeded":
+            sel.set_seed_step(1)
+
+
+def _tma_skip(variant, k_vals):
+    if variant.startswith("tma") and max(k_vals) > 64:
+        pytest.skip("the TMA-fed kernel handles k_max <= 64")
+
+
+def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, variant="auto", **kw):
     s = datagen.generate(n_train, n_val, p, n_mag=kw.pop("n_mag", 5), seed=seed, **kw)
     prob = oracle.Problem(s.Xtrain, s.ytrain, s.Xval, s.yval)
     o = oracle.select(prob, k_vals, nf, method)
     with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=k_vals, num_features=nf, method=method) as sel:
-        sel.set_kernel(kernel)
+        configure(sel, variant)
         r = sel.run()
     return o, r
 
@@ -112,14 +130,11 @@ def _holdout_case(n_train, n_val, p, seed, k_vals, nf, method, kernel=0, **kw):
     (1100, 333, 13, 14, [50, 33, 3], 5, "forward"),    # 64-slot lists, k_max 50
     (900, 250, 11, 15, [40], 5, "backward"),           # backward with 64-slot lists
 ])
-@pytest.mark.parametrize("kernel", [1, 2, 3])
-def test_holdout_matches_oracle(args, kernel):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_holdout_matches_oracle(args, variant):
     n_train, n_val, p, seed, kv, nf, method = args
-    if kernel == 2 and max(kv) > 64:
-        pytest.skip("the row-tile kernel handles k_max <= 64")
-    if kernel == 3 and max(kv) > 64:
-        pytest.skip("the TMA-fed kernel handles k_max <= 64")
-    o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method, kernel=kernel)
+    _tma_skip(variant, kv)
+    o, r = _holdout_case(n_train, n_val, p, seed, kv, nf, method, variant=variant)
     np.testing.assert_array_equal(r["ordering"], o["ordering"])
     np.testing.assert_array_equal(r["mask"], o["mask"])
     np.testing.assert_array_equal(r["errors"], o["errors"])
@@ -202,35 +217,34 @@ def test_headline_shape_subset_rows_against_oracle():
 
 
 @pytest.mark.parametrize("args", [
-    (8192, 2048, 40, 61, [10], 8, dict(n_heavy=6)),
-    (6000, 1500, 24, 62, [5, 50], 6, dict(mixture=True, dup_frac=0.02)),
+    (8192, 2048, 40, 61, [10], 9, dict(n_heavy=6)),
+    (6000, 1500, 24, 62, [5, 50], 7, dict(mixture=True, dup_frac=0.02)),
     (3000, 0, 20, 63, [3, 7], 6, dict()),          # CV mode (n_val=0 -> rows are the training points)
+    (2500, 700, 18, 64, [17, 31], 6, dict()),      # 32-slot lists
 ])
-def test_pruned_forward_equals_full_scan(args):
-    """Pruned forward steps (default) against the full scan of every column:
-    identical orderings, errors and neighbour lists, and the pruning prunes."""
+def test_seeded_bounds_equal_first_pass(args):
+    """Forward steps whose starting bounds come from the commit's seed columns
+    (from the second step on) against steps that always run the first pass:
+    identical orderings, errors and neighbour lists."""
     n_train, n_val, p, seed, kv, nf, kw = args
     s = datagen.generate(n_train, max(n_val, 1), p, n_mag=6, seed=seed, **kw)
     Xv, yv = (s.Xval, s.yval) if n_val else (None, None)
     out = {}
-    for prune in (True, False):
+    for seed_step in (1, 10 ** 6):
         with Selector(s.Xtrain, s.ytrain, Xv, yv, k_vals=kv, num_features=nf, method="forward", k_fold=5) as sel:
-            sel.set_pruning(prune)
+            sel.set_seed_step(seed_step)
             r = sel.run()
-            cnt = sel.counters()
             sel.reset()
-            for _ in range(3):
+            for _ in range(4):
                 sel.step()
             sel.keep_neighbours(True)
             sel.step()
-            out[prune] = (r, cnt, sel.neighbours())
-    (ra, ca, na), (rb, cb, nb) = out[True], out[False]
+            out[seed_step] = (r, sel.neighbours())
+    (ra, na), (rb, nb) = out[1], out[10 ** 6]
     for k in ("ordering", "mask", "errors", "errors64", "step_best_k"):
         np.testing.assert_array_equal(ra[k], rb[k])
     for a, b in zip(na, nb):
         np.testing.assert_array_equal(a, b)
-    assert ca["pairs_streamed"] > 0 and ca["pairs_survived"] < ca["pairs_streamed"]
-    assert cb["pairs_streamed"] == 0
 
 
 @pytest.mark.parametrize("kv", [[10], [50, 7]])
@@ -239,10 +253,12 @@ def test_large_problem_sampled_rows_match_oracle(kv):
     validation rows, mixture features, 2 % duplicated training rows): after
     three committed steps, the fourth step's neighbour lists of 96 sampled
     validation rows equal the oracle's, which recomputes those rows'
-    distances from X in commit order.  k = 10 runs the TMA-fed kernel,
-    k = 50 the row-tile kernel."""
+    distances from X in commit order.  Both k = 10 (16-slot lists) and
+    k = 50 (64-slot lists) run the TMA-fed kernel, the fourth step from seed
+    bounds when the seed step is 3."""
     s = datagen.generate(120000, 30000, 24, n_mag=8, seed=55, mixture=True, dup_frac=0.02)
     with Selector(s.Xtrain, s.ytrain, s.Xval, s.yval, k_vals=kv, num_features=4, method="forward") as sel:
+        sel.set_seed_step(3)
         for _ in range(3):
             assert sel.step()
         committed = [int(c) for c in sel.results()["ordering"][:3]]
@@ -298,7 +314,7 @@ def test_noalloc_backward_step_matches_handle():
     assert (c, k) == want[:2] and e == want[2]
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("case", [
     dict(n_train=300, n_val=70, p=2, kv=[3], nf=2, method="forward"),       # fewer candidates than a warp's four
     dict(n_train=260, n_val=50, p=3, kv=[2, 5], nf=1, method="backward"),
@@ -308,18 +324,17 @@ def test_noalloc_backward_step_matches_handle():
     dict(n_train=45, n_val=11, p=4, kv=[50, 2], nf=2, method="forward"),     # 64-slot lists, k > training rows
     dict(n_train=70, n_val=17, p=3, kv=[33], nf=2, method="backward"),
 ])
-def test_edge_shapes_match_oracle(case, kernel):
+def test_edge_shapes_match_oracle(case, variant):
     rng = np.random.default_rng(case["n_train"] * 7 + case["p"])
     Xt = rng.normal(size=(case["n_train"], case["p"])).astype(np.float32)
     Xv = rng.normal(size=(case["n_val"], case["p"])).astype(np.float32)
     yt = (Xt[:, 0] - 0.5 * Xt[:, -1] + rng.normal(0, 0.1, case["n_train"])).astype(np.float32)
     yv = (Xv[:, 0] - 0.5 * Xv[:, -1] + rng.normal(0, 0.1, case["n_val"])).astype(np.float32)
-    if kernel == 3 and max(case["kv"]) > 64:
-        pytest.skip("the TMA-fed kernel handles k_max <= 64")
+    _tma_skip(variant, case["kv"])
     prob = oracle.Problem(Xt, yt, Xv, yv)
     o = oracle.select(prob, case["kv"], case["nf"], case["method"])
     with Selector(Xt, yt, Xv, yv, k_vals=case["kv"], num_features=case["nf"], method=case["method"]) as sel:
-        sel.set_kernel(kernel)
+        configure(sel, variant)
         r = sel.run()
     np.testing.assert_array_equal(r["ordering"], o["ordering"])
     np.testing.assert_array_equal(r["mask"], o["mask"])
@@ -328,12 +343,11 @@ def test_edge_shapes_match_oracle(case, kernel):
     assert r["best_k"] == o["best_k"] and r["num_final"] == o["num_final"]
 
 
-@pytest.mark.parametrize("kernel", [0, 1])
-def test_forward_bound_overflow_and_ties(kernel):
-    """Forward steps after the first bound each list by its last neighbours'
-    distances under the new D.  A dominant feature whose squared differences
-    overflow to inf (selected first) leaves those distances non-finite, so the
-    bound falls back to none; quantized values give ties at the bound."""
+@pytest.mark.parametrize("variant", ["auto", "lanes", "tma_seeded"])
+def test_forward_bound_overflow_and_ties(variant):
+    """A dominant feature whose squared differences overflow to inf (selected
+    first) leaves the committed distances non-finite, so first-pass and seed
+    bounds are +inf (no bound); quantized values give ties at the bound."""
     rng = np.random.default_rng(77)
     n_train, n_val, p = 900, 260, 7
     Xt = rng.integers(-3, 4, size=(n_train, p)).astype(np.float32)
@@ -345,7 +359,7 @@ def test_forward_bound_overflow_and_ties(kernel):
     prob = oracle.Problem(Xt, yt, Xv, yv)
     o = oracle.select(prob, [1, 6, 21], 4, "forward")
     with Selector(Xt, yt, Xv, yv, k_vals=[1, 6, 21], num_features=4, method="forward") as sel:
-        sel.set_kernel(kernel)
+        configure(sel, variant)
         r = sel.run()
     assert o["ordering"][0] == 2
     np.testing.assert_array_equal(r["ordering"], o["ordering"])

@@ -38,12 +38,16 @@ def _winner(err32, err64, cands, k_vals):
     return best
 
 
-def test_noalloc_step_matches_handle_step_twice():
+@pytest.mark.parametrize("k_list", [[3, 7], [70, 4]])
+def test_noalloc_step_matches_handle_step_twice(k_list):
+    """k_max <= 64 runs the TMA-fed scorer, k_max 70 the rows-per-lane one.
+    The second call must not change the device's free memory (nothing is
+    allocated: the scratch was placed when the library's module loaded)."""
     import torch
 
     torch.cuda.init()
     s = datagen.generate(3000, 1000, 12, n_mag=5, n_heavy=2, seed=71)
-    k_vals = np.array([3, 7], np.int32)
+    k_vals = np.array(k_list, np.int32)
     n_tr, n_val, p = s.Xtrain.shape[0], s.Xval.shape[0], s.Xtrain.shape[1]
 
     # existing entry point: the handle API's first greedy step
@@ -69,12 +73,18 @@ def test_noalloc_step_matches_handle_step_twice():
 
     L = _lib.lib()
     results = []
-    for _ in range(2):
+    for call in range(2):
+        if call == 1:
+            free_before = torch.cuda.mem_get_info(dev)[0]
+            torch_before = torch.cuda.memory_allocated(dev)
         rc = L.snn_score_step_noalloc(D.data_ptr(), ld, XT.data_ptr(), XV.data_ptr(), n_val, yt.data_ptr(),
                                       yv.data_ptr(), n_val, n_tr, p, ptr(cands, _i32p), p, ptr(k_vals, _i32p),
                                       k_vals.size, 0, err32.data_ptr(), err64.data_ptr(),
                                       ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, _lib.last_error()
+        if call == 1:
+            assert torch.cuda.mem_get_info(dev)[0] == free_before
+            assert torch.cuda.memory_allocated(dev) == torch_before
         e32, e64 = err32.cpu().numpy().copy(), err64.cpu().numpy().copy()
         got = _winner(e32, e64, cands, k_vals)
         assert got[1] == want[1] and got[2] == want[2]
@@ -94,3 +104,16 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                   ptr(k_vals, _i32p), 1, 0, 1, 1, None)
     assert rc == _lib.SNN_ERR_ARG
     assert b"scratch" in L.snn_last_error()
+
+
+def test_noalloc_rejects_misaligned_device_pointers():
+    """D and XT are read by TMA copies, which need 16-byte aligned bases: a
+    misaligned pointer is refused up front with a message that says so (no
+    kernel is launched, so the pointers are never dereferenced)."""
+    L = _lib.lib()
+    k_vals = np.array([5], np.int32)
+    cands = np.arange(4, dtype=np.int32)
+    rc = L.snn_score_step_noalloc(256 + 4, 64, 256, 256, 64, 256, 256, 64, 64, 4, ptr(cands, _i32p), 4,
+                                  ptr(k_vals, _i32p), 1, 0, 256, 256, None)
+    assert rc == _lib.SNN_ERR_ARG
+    assert b"16-byte aligned" in L.snn_last_error()
