@@ -8,7 +8,7 @@ from conftest import ROOT, golden_cases
 from oracle import oracle, ref
 
 GDIR = os.path.join(ROOT, "tests", "golden")
-SELECT_CASES = [n for n in golden_cases() if not n.startswith(("nn_", "model_")) and n != "losses"]
+SELECT_CASES = [n for n in golden_cases() if not n.startswith(("nn_", "model_", "config_")) and n != "losses"]
 NN_CASES = golden_cases("nn_")
 
 
