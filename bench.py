@@ -16,8 +16,18 @@ ours:       inputs resident in HBM; each step = snn_run (initial distance
 reference:  speedynn's own CPU neighbour scan (get_k_nearest_neighbors_cpu,
             speedynn/lib/cpu.c:128-168, compiled from the reference sources
             into oracle/_ref) on a bounded sample of the same workload:
-            sampled validation rows x all 65,536 training rows x all 60
-            candidates of the first step, one process per host core.
+            sampled validation rows x all 65,536 training rows x the 53
+            candidates of the eighth greedy step (the first seven features
+            committed into the sampled rows' distances), one process per host
+            core.  ms_per_step is the measured time of one such sample.
+
+Besides the timed loop, the default run (one GPU, rank 0) also reports:
+  oracle      the selection against the full-size oracle fixture of the same
+              workload (tests/golden/config_*.npz: ordering and FP32 errors
+              bit for bit, and each FP32 error against the all-FP64 pipeline);
+  batched     the batch workload (320 problems) run once as one batch and once
+              as the plain single-problem form, with identical results checked;
+  cpu_baseline  the reference CPU scan on a bounded sample (as --impl reference).
 
 N > 1 (torchrun): every rank runs its own selection problem (seed offset by
 rank): independent problems, no collective on the data path; value sums all
@@ -83,6 +93,53 @@ def scoring_kernel(kmax, option=0):
     return "k_score"
 
 
+# FP32-pipe operations per evaluation in the roofline's work count: sub, mul,
+# add and compare (the reference's scalar loop); the scorer's filter issues one
+# packed sub and one packed FMA per evaluation plus a sign-bit OR.
+OPS_PER_EVAL = 4
+
+
+def fixture_path(name):
+    return os.path.join(ROOT, "tests", "golden", f"config_{name.replace('-', '')}.npz")
+
+
+def data_sha256(split):
+    import hashlib
+    h = hashlib.sha256()
+    for a in (split.Xtrain, split.ytrain, split.Xval, split.yval):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def oracle_statement(name, split, res):
+    """The run's selection against the committed full-size oracle fixture of
+    the same workload (tests/golden/make_config_golden.py): ordering and FP32
+    errors bit for bit over the fixture's steps, FP64 errors against the
+    oracle's FP64 sums, and each FP32 error against the all-FP64 pipeline."""
+    path = fixture_path(name)
+    if not os.path.exists(path):
+        return {"available": False, "why": f"no fixture {os.path.basename(path)}"}
+    g = np.load(path)
+    if str(g["data_sha256"]) != data_sha256(split):
+        return {"available": False, "why": "generated inputs differ from the fixture's (generator changed)"}
+    slots = [int(x) for x in g["slots"]]
+    e32 = np.array([res["errors"][i] for i in slots], np.float32)
+    o32 = np.array([g["errors"][i] for i in slots], np.float32)
+    e64 = np.array([res["errors64"][i] for i in slots])
+    o64 = np.array([g["errors64"][i] for i in slots])
+    pipe = np.asarray(g["errors_fp64_pipeline"], np.float64)
+    gap = np.abs(e32.astype(np.float64) - pipe) / pipe
+    return {"available": True, "fixture": os.path.basename(path), "steps_compared": len(slots),
+            "ordering_equal": bool(all(res["ordering"][i] == g["ordering"][i] for i in slots)),
+            "errors_bit_equal": bool(np.array_equal(e32, o32)),
+            "errors64_max_rel_vs_oracle": float(np.max(np.abs(e64 - o64) / o64)),
+            "fp32_vs_fp64_pipeline": {"max_rel": float(gap.max()), "per_step_rel": [float(x) for x in gap],
+                                      "fp64_pipeline": [float(x) for x in pipe]},
+            "note": "fp64_pipeline = RMSE of each step's winner with FP64 distances, FP64 neighbour order and "
+                    "FP64 predictions (oracle, all rows); max_rel = largest |FP32 error - FP64 pipeline| / FP64 "
+                    "pipeline over the steps"}
+
+
 def cand_evals(n_rows, n_cols, p, steps):
     return float(n_rows) * n_cols * sum(p - t for t in range(steps))
 
@@ -144,12 +201,13 @@ class Clocks:
 _W = {}
 
 
-def _ref_worker_init(npz_path, k):
+def _ref_worker_init(npz_path, k, committed):
     import ctypes
     from oracle import ref
     d = np.load(npz_path)
     _W["Xv"], _W["yv"], _W["Xt"], _W["yt"] = d["Xval"], d["yval"], d["Xtrain"], d["ytrain"]
     _W["k"] = k
+    _W["committed"] = list(committed)
     _W["lib"] = ref.load()
     _W["ct"] = ctypes
 
@@ -158,7 +216,10 @@ def _ref_worker_run(rows):
     """Holdout scoring of validation rows ``rows`` with the reference's own
     get_k_nearest_neighbors_cpu: the rows are placed in front of the training
     block as fold 0 (num_per_fold = len(rows)), so each scans exactly the
-    training points; then the kNN mean and squared error as cpu.c:56-66."""
+    training points; then the kNN mean and squared error as cpu.c:56-66.
+    The rows' distances hold the committed features, summed in commit order
+    with the reference's rounding (cpu.c:217-231), and every other feature is
+    a candidate."""
     ct = _W["ct"]
     L = _W["lib"]
     Xv, yv, Xt, yt, k = _W["Xv"], _W["yv"], _W["Xt"], _W["yt"], _W["k"]
@@ -166,7 +227,11 @@ def _ref_worker_run(rows):
     Xp = np.ascontiguousarray(np.concatenate([Xv[rows], Xt]), np.float32)
     yp = np.concatenate([yv[rows], yt]).astype(np.float32)
     n, p = Xp.shape
-    D = np.zeros((R, n), np.float32)  # step 0 of forward selection: empty committed set
+    D = np.zeros((R, n), np.float32)
+    for w in _W["committed"]:
+        t = (Xp[:R, w][:, None] - Xp[None, :, w]).astype(np.float32)
+        D = (D + (t * t).astype(np.float32)).astype(np.float32)
+    cands = [c for c in range(p) if c not in _W["committed"]]
     ib = np.zeros(k, np.int32)
     db = np.zeros(k, np.float32)
     ip = ib.ctypes.data_as(ct.POINTER(ct.c_int))
@@ -178,7 +243,7 @@ def _ref_worker_run(rows):
     ct.c_void_p.in_dll(L, "current_dist_matrix").value = D.ctypes.data
     sse = np.zeros(p, np.float64)
     t0 = time.perf_counter()
-    for c in range(p):
+    for c in cands:
         for r in range(R):
             L.get_k_nearest_neighbors_cpu(r, 0, R, ip, dp, c, 1)
             pred = np.float32(yp[ib].sum(dtype=np.float32) / np.float32(k))
@@ -186,19 +251,21 @@ def _ref_worker_run(rows):
     el = time.perf_counter() - t0
     ct.c_void_p.in_dll(L, "current_dist_matrix").value = None
     ct.c_void_p.in_dll(L, "training_patterns").value = None
-    return el, float(R) * Xt.shape[0] * p
+    return el, float(R) * Xt.shape[0] * len(cands)
 
 
 class RefCPU:
     """Process pool timing the reference's CPU scan; one process per core."""
 
-    def __init__(self, split, k, rows_per_proc, procs=None):
+    def __init__(self, split, k, rows_per_proc, committed=(), procs=None):
         import multiprocessing as mp
         self.procs = procs or len(os.sched_getaffinity(0))
         fd, self.npz = tempfile.mkstemp(suffix=".npz")
         os.close(fd)
         np.savez(self.npz, Xval=split.Xval, yval=split.yval, Xtrain=split.Xtrain, ytrain=split.ytrain)
-        self.pool = mp.get_context("spawn").Pool(self.procs, initializer=_ref_worker_init, initargs=(self.npz, k))
+        self.committed = list(committed)
+        self.pool = mp.get_context("spawn").Pool(self.procs, initializer=_ref_worker_init,
+                                                 initargs=(self.npz, k, self.committed))
         self.rows = rows_per_proc
         self.nval = split.Xval.shape[0]
         self.calls = 0
@@ -226,15 +293,31 @@ def ref_available():
     return os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libspeedynn_ref.so"))
 
 
-def port_cpu_rate(split, k, rows):
+def port_cpu_rate(split, k, rows, committed=()):
     """Fallback CPU baseline: the oracle restatement (OpenMP, all cores)."""
     from oracle import oracle
     prob = oracle.Problem(split.Xtrain, split.ytrain, split.Xval, split.yval)
     p = split.Xtrain.shape[1]
+    cands = [c for c in range(p) if c not in committed]
     t0 = time.perf_counter()
-    oracle.step(prob, [k], [], list(range(p)), rows=list(range(rows)), want_neighbours=False)
+    oracle.step(prob, [k], list(committed), cands, rows=list(range(rows)), want_neighbours=False)
     el = time.perf_counter() - t0
-    return float(rows) * split.Xtrain.shape[0] * p / el, el
+    return float(rows) * split.Xtrain.shape[0] * len(cands) / el, el
+
+
+# The reference arm and the CPU baseline sample the eighth greedy step: the
+# first seven winners of the fwd-64k oracle fixture are committed (the first
+# seven features otherwise), leaving 53 candidates, the selection's average.
+REF_COMMITTED = 7
+
+
+def ref_committed(name, split):
+    path = fixture_path(name)
+    if os.path.exists(path):
+        g = np.load(path)
+        if str(g["data_sha256"]) == data_sha256(split):
+            return [int(x) for x in g["commit_order"][:REF_COMMITTED]]
+    return list(range(REF_COMMITTED))
 
 
 # ---------------------------------------------------------------------------
@@ -251,12 +334,14 @@ def run_reference(args, world, rank):
         return 0
     split, k, steps = datagen.workload(WORKLOAD)
     n_train, n_val, p = split.Xtrain.shape[0], split.Xval.shape[0], split.Xtrain.shape[1]
-    cfg = workload_desc(k, steps, n_train, n_val, p)
+    cfg = dict(workload_desc(k, steps, n_train, n_val, p), parallelism=f"independent problems x{world}")
     line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": cfg}
+    committed = ref_committed(WORKLOAD, split)
+    n_cand = p - len(committed)
     if ref_available():
-        rc = RefCPU(split, k, args.ref_rows)
+        rc = RefCPU(split, k, args.ref_rows, committed)
         for _ in range(args.warmup):
             rc.step()
         tot_e, tot_t = 0.0, 0.0
@@ -268,16 +353,21 @@ def run_reference(args, world, rank):
         v = tot_e / tot_t
         kind = "reference"
         sample = (f"speedynn get_k_nearest_neighbors_cpu + kNN mean, {rc.procs} processes x {args.ref_rows} "
-                  f"validation rows x {n_train} training rows x {p} candidates (first greedy step) per bench step")
+                  f"validation rows x {n_train} training rows x {n_cand} candidates (greedy step "
+                  f"{len(committed) + 1}, {len(committed)} features committed) per bench step")
         cores = rc.procs
     else:
-        v, el = port_cpu_rate(split, k, args.ref_rows)
+        el_tot = 0.0
+        for _ in range(args.steps):
+            v, el = port_cpu_rate(split, k, args.ref_rows, committed)
+            el_tot += el
+        tot_t = el_tot
         kind = "port"
         cores = len(os.sched_getaffinity(0))
-        sample = f"oracle restatement, {args.ref_rows} validation rows x {n_train} x {p} candidates"
-        tot_t = el * args.steps
-    line.update({"value": v, "ms_per_step": 1000.0 * cand_evals(n_val, n_train, p, steps) / v,
-                 "ms_per_step_note": "extrapolated: full 15-step selection at the measured CPU rate",
+        sample = f"oracle restatement, {args.ref_rows} validation rows x {n_train} x {n_cand} candidates"
+    line.update({"value": v, "ms_per_step": 1000.0 * tot_t / max(1, args.steps),
+                 "ms_per_step_note": "measured: one bounded sample (see cpu_baseline.sample) per bench step",
+                 "ms_full_selection_extrapolated": 1000.0 * cand_evals(n_val, n_train, p, steps) / v,
                  "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
                  "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                  "gpu_launches": 0})
@@ -376,7 +466,7 @@ def run_ours(args, world, rank, local):
     e2e_s = allmax((time.perf_counter() - e0) / args.steps, world)
     sel.close()
 
-    # roofline of the scoring kernel: FP32 pipe (3 rounded ops per evaluation) vs one D read
+    # roofline of the scoring kernel: FP32 pipe (OPS_PER_EVAL ops per evaluation) vs one D read
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -389,7 +479,7 @@ def run_ours(args, world, rank, local):
     fp32_peak = sm * 128 * mhz * 1e6 * 1e-12  # T ops/s of the FP32 pipe at the sampled clock
     avg_score_s = score_ms / max(1, score_n) / 1000.0
     evals_per_launch = evals / steps
-    achieved_fp32 = 3.0 * evals_per_launch / avg_score_s * 1e-12
+    achieved_fp32 = OPS_PER_EVAL * evals_per_launch / avg_score_s * 1e-12
     bytes_per_launch = 4.0 * n_val * n_train
     achieved_hbm = bytes_per_launch / avg_score_s * 1e-9
 
@@ -413,8 +503,14 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "fp32", "kernel": scoring_kernel(k, args.kernel), "achieved": achieved_fp32,
                          "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved_fp32 / fp32_peak,
-                         "peak_source": f"{sm} SMs x 128 FP32 lanes x {mhz:.0f} MHz (sampled median; no FP32 "
-                                        "figure in MEASURED_PEAKS.json); work = 3 rounded FP32 ops per evaluation",
+                         "ops_per_eval": OPS_PER_EVAL,
+                         "frac_3op": 0.75 * achieved_fp32 / fp32_peak,
+                         "evals_per_s_per_launch": evals_per_launch / avg_score_s,
+                         "launch_ms": avg_score_s * 1000.0,
+                         "peak_source": f"{sm} SMs x 128 FP32 lanes x {mhz:.0f} MHz (sampled median; "
+                                        "MEASURED_PEAKS.json holds no FP32 figure); work = 4 FP32-pipe ops per "
+                                        "evaluation (sub, mul, add, compare); frac_3op counts the 3 rounded "
+                                        "arithmetic ops only",
                          "hbm_achieved_gbs": achieved_hbm, "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src,
                          "hbm_frac": achieved_hbm / hbm,
                          "traffic": args.traffic if args.traffic is not None else TRAFFIC_PER_PAIR * n_val * n_train,
@@ -427,18 +523,25 @@ def run_ours(args, world, rank, local):
     if name != WORKLOAD:
         line["metric"] = METRIC.replace("greedy forward selection", "greedy backward elimination" if backward else
                                         "greedy forward selection") + f" ({name})"
+    if rank == 0 and world == 1 and args.rows_scale == 1.0 and not args.no_oracle:
+        line["oracle"] = oracle_statement(name, split, res)
+    if rank == 0 and world == 1 and name == WORKLOAD and args.rows_scale == 1.0 and not args.no_batch:
+        line["batched"] = batch_summary(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and name == WORKLOAD:
+        committed = ref_committed(name, split)
+        n_cand = p - len(committed)
         if ref_available():
-            rc = RefCPU(split, k, args.cpu_rows)
+            rc = RefCPU(split, k, args.cpu_rows, committed)
             e, t = rc.step()
             rc.close()
             line["cpu_baseline"] = {"value": e / t, "unit": UNIT, "cores": rc.procs, "kind": "reference",
-                                    "sample": f"speedynn get_k_nearest_neighbors_cpu, {rc.procs} processes x "
-                                              f"{args.cpu_rows} validation rows x {n_train} x {p} candidates"}
+                                    "sample": f"speedynn get_k_nearest_neighbors_cpu + kNN mean, {rc.procs} "
+                                              f"processes x {args.cpu_rows} validation rows x {n_train} x {n_cand} "
+                                              f"candidates (greedy step {len(committed) + 1})"}
         else:
-            v, el = port_cpu_rate(split, k, args.cpu_rows)
+            v, el = port_cpu_rate(split, k, args.cpu_rows, committed)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": len(os.sched_getaffinity(0)), "kind": "port",
-                                    "sample": f"oracle restatement, {args.cpu_rows} rows x {n_train} x {p}"}
+                                    "sample": f"oracle restatement, {args.cpu_rows} rows x {n_train} x {n_cand}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -463,6 +566,35 @@ def run_plain(probs, batch_res, evals, batch_ms, world):
     return {"ms": plain_ms, "value": world * evals / (plain_ms / 1000.0), "batched_speedup": plain_ms / batch_ms,
             "identical_results": bool(same),
             "note": "the problems one at a time (CUDA-event time of each selection, creates and uploads excluded)"}
+
+
+def batch_summary(args, local):
+    """Batched vs plain on the batch workload (320 holdout problems), outside
+    the timed loop of the default line: one warm-up batch, one measured batch
+    (device time and end to end through snn_batch_*), then the same problems
+    one at a time through the handle API, results compared."""
+    from speedynn_b200 import datagen
+    from speedynn_b200.batch import Batch
+
+    probs = datagen.batch_workload(seed0=4000)
+    evals = sum(cand_evals(pr["Xval"].shape[0], pr["Xtrain"].shape[0], pr["Xtrain"].shape[1], pr["num_features"])
+                for pr in probs)
+    b = Batch(probs)
+    b.run()
+    t0 = time.perf_counter()
+    res = b.run()
+    wall = time.perf_counter() - t0
+    tm = b.timing()
+    b.close()
+    plain = run_plain(probs, res, evals, tm["run_ms"], 1)
+    return {"workload": f"batch-64x5: {len(probs)} holdout forward selections, n_train 1,045..30,790, p=40, "
+                        "k in {1,5,10,20}, 15 steps", "evals": evals,
+            "batch_ms": tm["run_ms"], "batch_value": evals / (tm["run_ms"] / 1000.0),
+            "batch_e2e_value": evals / wall, "batch_e2e_ms": 1000.0 * wall,
+            "plain_ms": plain["ms"], "plain_value": plain["value"], "batched_speedup": plain["batched_speedup"],
+            "identical_results": plain["identical_results"],
+            "note": "batch_ms: union of the problems' CUDA-event intervals; batch_e2e: snn_batch_run wall time "
+                    "(creates, uploads, runs, result reads, frees); plain: each problem's own selection time"}
 
 
 def run_batch(args, world, rank, local):
@@ -533,6 +665,9 @@ def main():
     ap.add_argument("--kernel", type=int, default=0, help="scoring kernel: 0 auto, 1 rows per lane, 3 TMA-fed row tiles")
     ap.add_argument("--seed-step", type=int, default=None,
                     help="first forward step scored from seed bounds (library option; default: the library's)")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the comparison with the full-size oracle fixture")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batch-vs-plain comparison that the default workload's line carries")
     ap.add_argument("--workload", default=WORKLOAD,
                     choices=["fwd-64k", "bwd-50k", "fwd-200k", "batch-64x5"],
                     help="fwd-64k (the headline), bwd-50k (backward, p=120 -> 20), fwd-200k (80 GB distance matrix, "
