@@ -110,6 +110,8 @@ struct snn_handle {
     bool loaded = false;
     int host_step = 0;  // steps issued since the last reset
     // timing
+    bool step_events = true;  // per-step CUDA events (off for batch problems: only total_ev is read)
+    bool arena = false;       // device buffers are sub-allocations of a batch arena (never freed one by one)
     std::vector<EventPair> score_ev, commit_ev;
     EventPair total_ev;
     int n_score = 0, n_commit = 0, n_launch = 0;
@@ -170,12 +172,31 @@ namespace {
 //                             of stage N, so its bounded waits run out (SNN_ERR_TIMEOUT)
 thread_local int t_fail_alloc = 0;  // countdown to the injected allocation failure, 0 = off
 
+// Bump allocator over one device allocation: while a batch creates and loads
+// the problems of a wave on this thread, their buffers are carved from it
+// (one cudaMalloc per batch run instead of a score per problem; cudaFree
+// also waits for the whole device).  256-byte aligned sub-allocations.
+struct Arena {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+};
+thread_local Arena *t_arena = nullptr;
+
 template <typename T>
 int dev_alloc(T **p, size_t n, const char *what)
 {
     *p = nullptr;
     if (t_fail_alloc > 0 && --t_fail_alloc == 0) return fail(SNN_ERR_NOMEM, "injected failure of the allocation of %s", what);
     if (n == 0) n = 1;
+    if (t_arena) {
+        const size_t off = (t_arena->used + 255) & ~(size_t)255;
+        const size_t bytes = n * sizeof(T);
+        if (off > t_arena->cap || bytes > t_arena->cap - off)
+            return fail(SNN_ERR_NOMEM, "batch arena full at %s (%zu bytes)", what, bytes);
+        *p = reinterpret_cast<T *>(t_arena->base + off);
+        t_arena->used = off + bytes;
+        return SNN_OK;
+    }
     cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
     if (e != cudaSuccess) {
         *p = nullptr;
@@ -189,12 +210,14 @@ int dev_alloc(T **p, size_t n, const char *what)
 void free_all(snn_handle *h)
 {
     cudaSetDevice(h->device);
-    void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
-                    h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                    h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->perm, h->fvar,
-                    h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
-    for (void *q : ptrs)
-        if (q) cudaFree(q);
+    if (!h->arena) {  // an arena's buffers are freed by its owner
+        void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
+                        h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
+                        h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->perm, h->fvar,
+                        h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
+        for (void *q : ptrs)
+            if (q) cudaFree(q);
+    }
     for (auto &e : h->score_ev) {
         if (e.a) cudaEventDestroy(e.a);
         if (e.b) cudaEventDestroy(e.b);
@@ -253,10 +276,13 @@ int issue_step(snn_handle *h, int t)
     const int n_cand = h->p - t;  // forward: p - t unselected; backward: p - t still selected
     const int backward = h->desc.backward;
     const int it = backward ? h->p - 1 - t : t;
-    if ((int)h->score_ev.size() <= h->n_score) h->score_ev.resize(h->n_score + 1);
-    EventPair &se = h->score_ev[h->n_score];
-    if (int rc = make_pair(se)) return rc;
-    SNN_CUDA(cudaEventRecord(se.a, h->stream));
+    EventPair *se = nullptr;
+    if (h->step_events) {
+        if ((int)h->score_ev.size() <= h->n_score) h->score_ev.resize(h->n_score + 1);
+        se = &h->score_ev[h->n_score];
+        if (int rc = make_pair(*se)) return rc;
+        SNN_CUDA(cudaEventRecord(se->a, h->stream));
+    }
     if (t == h->inject_launch) {
         h->inject_launch = -1;
         return fail(SNN_ERR_CUDA, "injected launch failure at step %d", t);
@@ -273,9 +299,11 @@ int issue_step(snn_handle *h, int t)
     } else {
         SNN_CUDA(snn::launch_score(b, n_cand, h->plan, backward, h->stream));
     }
-    SNN_CUDA(cudaEventRecord(se.b, h->stream));
+    if (se) {
+        SNN_CUDA(cudaEventRecord(se->b, h->stream));
+        h->n_score++;
+    }
     if (!tma_step) h->prev_ok = false;
-    h->n_score++;
     if (h->model == 1) {
         SNN_CUDA(snn::launch_mode_predict(b, n_cand, h->stream));
         h->n_launch += 1;
@@ -290,15 +318,20 @@ int issue_step(snn_handle *h, int t)
     if (h->keep_nn) h->nn_ncand = n_cand;
     h->last_ncand = n_cand;
     if (t + 1 < h->total_steps) {
-        if ((int)h->commit_ev.size() <= h->n_commit) h->commit_ev.resize(h->n_commit + 1);
-        EventPair &ce = h->commit_ev[h->n_commit];
-        if (int rc = make_pair(ce)) return rc;
-        SNN_CUDA(cudaEventRecord(ce.a, h->stream));
+        EventPair *ce = nullptr;
+        if (h->step_events) {
+            if ((int)h->commit_ev.size() <= h->n_commit) h->commit_ev.resize(h->n_commit + 1);
+            ce = &h->commit_ev[h->n_commit];
+            if (int rc = make_pair(*ce)) return rc;
+            SNN_CUDA(cudaEventRecord(ce->a, h->stream));
+        }
         const bool sd = seeds_for_step(h, t + 1);
         SNN_CUDA(snn::launch_commit(b, backward, sd ? h->seeds : nullptr, sd ? h->seed_d : nullptr, h->stream));
         h->seeds_ok = sd;
-        SNN_CUDA(cudaEventRecord(ce.b, h->stream));
-        h->n_commit++;
+        if (ce) {
+            SNN_CUDA(cudaEventRecord(ce->b, h->stream));
+            h->n_commit++;
+        }
         h->n_launch += 1;
     }
     return SNN_OK;
@@ -397,6 +430,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (int rc = check_device(d->device)) return rc;
 
     snn_handle *h = new snn_handle();
+    h->arena = t_arena != nullptr;  // a batch creating this handle from its arena
     if (const char *f = getenv("SNN_INJECT_FAIL")) {
         if (!strncmp(f, "alloc:", 6)) t_fail_alloc = atoi(f + 6);
         if (!strncmp(f, "launch:", 7)) h->inject_launch = atoi(f + 7);
@@ -498,7 +532,7 @@ static int load_matrix(snn_handle *h, const float *X, int n, float *XT, int ld, 
 }
 
 static int load_impl(snn_handle *h, const float *X_train, const float *y_train, const float *X_val,
-                     const float *y_val, bool device_src)
+                     const float *y_val, bool device_src, bool wait = true)
 {
     g_err.clear();
     if (!h) return fail(SNN_ERR_ARG, "null handle");
@@ -517,21 +551,14 @@ static int load_impl(snn_handle *h, const float *X_train, const float *y_train, 
     // candidates a scoring warp shares a filter bound with have distances of
     // similar scale (any order gives the same results)
     SNN_CUDA(snn::launch_feature_variance(h->bufs(), h->fvar, h->stream));
-    std::vector<float> var(h->p);
-    SNN_CUDA(cudaMemcpyAsync(var.data(), h->fvar, sizeof(float) * h->p, cudaMemcpyDeviceToHost, h->stream));
-    SNN_CUDA(cudaStreamSynchronize(h->stream));
-    std::vector<int> perm(h->p);
-    for (int j = 0; j < h->p; ++j) perm[j] = j;
-    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
-        const bool na = std::isnan(var[a]), nb = std::isnan(var[b]);
-        if (na != nb) return nb;  // non-finite columns last
-        return !na && var[a] < var[b];
-    });
-    SNN_CUDA(cudaMemcpyAsync(h->perm, perm.data(), sizeof(int) * h->p, cudaMemcpyHostToDevice, h->stream));
+    SNN_CUDA(snn::launch_feature_order(h->fvar, h->p, h->perm, h->stream));
     h->loaded = true;
     reset_timing(h);
     if (int rc = issue_reset(h)) return rc;
-    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    // A batch issues the selection on the same stream right away (its inputs
+    // stay valid until the batch run returns); a single load waits, so the
+    // caller may reuse pinned source buffers at once.
+    if (wait) SNN_CUDA(cudaStreamSynchronize(h->stream));
     return SNN_OK;
 }
 
@@ -1042,6 +1069,16 @@ SNN_API int snn_batch_run(snn_batch *B)
             const size_t reserve = std::max<size_t>((size_t)1 << 30, tot / 50);
             budget = fr > reserve ? fr - reserve : 0;
         }
+        // the wave's buffers come from one device allocation of the budget
+        // (without it, from cudaMalloc per buffer)
+        Arena arena;
+        void *abase = nullptr;
+        if (budget > 0 && cudaMalloc(&abase, budget) == cudaSuccess) {
+            arena.base = static_cast<char *>(abase);
+            arena.cap = budget;
+        } else {
+            cudaGetLastError();
+        }
         std::vector<snn_handle *> hs;
         size_t used = 0;
         const int i0 = i;
@@ -1053,7 +1090,14 @@ SNN_API int snn_batch_run(snn_batch *B)
             if (!hs.empty() && used + need > budget) break;
             snn_handle *h = nullptr;
             const snn_batch::Problem &P = B->prob[i];
-            if ((rc = snn_create(&P.desc, &h)) || (rc = snn_load(h, P.Xt, P.yt, P.Xv, P.yv))) {
+            t_arena = arena.base ? &arena : nullptr;
+            rc = snn_create(&P.desc, &h);
+            if (rc == SNN_OK) {
+                h->step_events = false;  // only the selection's total events are read (finish_wave)
+                rc = load_impl(h, P.Xt, P.yt, P.Xv, P.yv, false, false);
+            }
+            t_arena = nullptr;
+            if (rc) {
                 snn_destroy(h);
                 if (rc == SNN_ERR_NOMEM && !hs.empty()) {
                     rc = SNN_OK;  // run what fits, retry this problem in the next wave
@@ -1069,6 +1113,7 @@ SNN_API int snn_batch_run(snn_batch *B)
         }
         if (rc == SNN_OK && !hs.empty()) rc = finish_wave(B, hs, i0);
         for (snn_handle *h : hs) snn_destroy(h);
+        if (abase) cudaFree(abase);
         if (rc) return fail(rc, "snn_batch_run, problem %d: %s", i, std::string(g_err).c_str());
     }
     return SNN_OK;

@@ -118,6 +118,8 @@ cudaError_t launch_losses(const Bufs &b, int n_cand, cudaStream_t s);
 cudaError_t launch_row_dmax(const Bufs &b, float *dmax, cudaStream_t s);
 // Per-feature training variance (FP64 sums) into var[p], NaN for non-finite columns.
 cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s);
+// perm[0..p) = features by ascending var (NaN last, ties by id): the candidate slot order.
+cudaError_t launch_feature_order(const float *var, int p, int *perm, cudaStream_t s);
 cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, int backward, cudaStream_t s);
 
 }  // namespace snn

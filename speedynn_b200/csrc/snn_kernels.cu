@@ -358,6 +358,28 @@ __global__ void k_feature_variance(Bufs b, float *var)
     }
 }
 
+// Stable ascending order of the feature variances, NaN last: each thread
+// ranks one feature by counting the features that precede it (O(p^2), p is
+// the number of features).
+__global__ void k_feature_order(const float *var, int p, int *perm)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p; j += gridDim.x * blockDim.x) {
+        const float vj = var[j];
+        const bool nj = isnan(vj);
+        int rank = 0;
+        for (int i = 0; i < p; ++i) {
+            const float vi = var[i];
+            const bool ni = isnan(vi);
+            bool before;
+            if (ni != nj) before = nj;    // finite before NaN
+            else if (ni) before = i < j;  // both NaN: by id
+            else before = vi < vj || (vi == vj && i < j);
+            rank += before ? 1 : 0;
+        }
+        perm[rank] = j;
+    }
+}
+
 int sm_count()
 {
     // initialised once, thread-safely (handles may be created from several threads)
@@ -416,6 +438,12 @@ cudaError_t launch_force(const Bufs &b, int w, int it, int t, int total_steps, i
 cudaError_t launch_feature_variance(const Bufs &b, float *var, cudaStream_t s)
 {
     k_feature_variance<<<b.p, 256, 0, s>>>(b, var);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_feature_order(const float *var, int p, int *perm, cudaStream_t s)
+{
+    k_feature_order<<<(p + 127) / 128, 128, 0, s>>>(var, p, perm);
     return cudaGetLastError();
 }
 
