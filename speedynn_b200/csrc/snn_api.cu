@@ -96,6 +96,7 @@ struct snn_handle {
     // commit before a seeded step) and their distances, [n_rows][kSeeds]
     int *seeds = nullptr;
     float *seed_d = nullptr;
+    float *sbound = nullptr;      // [p][n_rows] starting bounds of a seeded step
     bool seeds_ok = false;        // seeds hold the current D's seed columns
     int seed_step = 4;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds
     unsigned long long *fcount = nullptr;  // filter counters of the TMA-fed scorer (3)
@@ -158,6 +159,7 @@ struct snn_handle {
         b.fcount = count_filter ? fcount : nullptr;
         b.seeds = seeds;
         b.seed_d = seed_d;
+        b.bound = sbound;
         b.use_seeds = 0;
         return b;
     }
@@ -213,7 +215,7 @@ void free_all(snn_handle *h)
     if (!h->arena) {  // an arena's buffers are freed by its owner
         void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                         h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                        h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->perm, h->fvar,
+                        h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->sbound, h->perm, h->fvar,
                         h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
         for (void *q : ptrs)
             if (q) cudaFree(q);
@@ -293,6 +295,10 @@ int issue_step(snn_handle *h, int t)
         b.use_seeds = seeds_for_step(h, t) && h->seeds_ok ? 1 : 0;
         b.inject_stall = h->inject_stall + 1;  // 0: off
         h->inject_stall = -1;
+        if (b.use_seeds) {
+            SNN_CUDA(snn::launch_seed_bounds(b, n_cand, h->stream));
+            h->n_launch += 1;
+        }
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
         h->prev_ok = backward && h->kth_prev;  // this step wrote every candidate's k-th distances
         tma_step = true;
@@ -410,7 +416,7 @@ static size_t handle_bytes(const snn_desc *d, int kmax)
     const size_t n_rows = cv ? n_cols : (size_t)d->n_val;
     const size_t ldc = (size_t)round_up(d->n_train, snn::kPadCols);
     const size_t ldr = cv ? ldc : (size_t)round_up((int)n_rows, snn::kPadCols);
-    const size_t M = d->backward ? 0 : 2 * (size_t)snn::kSeeds;  // seed columns and distances
+    const size_t M = d->backward ? 0 : 2 * (size_t)snn::kSeeds + p;  // seed columns, distances, bounds
     (void)kmax;
     size_t f = p * ldc + n_rows * ldc + p * (size_t)d->num_k_vals * n_rows + std::max(n_rows, n_cols) * p +
                n_rows * M + n_cols + n_rows;
@@ -502,6 +508,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (!d->backward) {
         if ((rc = dev_alloc(&h->seeds, (size_t)h->n_rows * snn::kSeeds, "seed columns"))) return bail(rc);
         if ((rc = dev_alloc(&h->seed_d, (size_t)h->n_rows * snn::kSeeds, "seed distances"))) return bail(rc);
+        if ((rc = dev_alloc(&h->sbound, p * h->n_rows, "seed bounds"))) return bail(rc);
     }
     // On the handle's stream, so every kernel that reads k_vals comes after it
     // (the source lives as long as the handle).  A cudaMemcpy here would run on
@@ -1071,11 +1078,15 @@ SNN_API int snn_batch_run(snn_batch *B)
         }
         // the wave's buffers come from one device allocation of the budget
         // (without it, from cudaMalloc per buffer)
+        // (a wave always admits its first problem, whatever the budget)
+        int kmax0 = 0;
+        validate_desc(&B->prob[i].desc, &kmax0);
+        const size_t cap = std::max(budget, handle_bytes(&B->prob[i].desc, kmax0));
         Arena arena;
         void *abase = nullptr;
-        if (budget > 0 && cudaMalloc(&abase, budget) == cudaSuccess) {
+        if (cudaMalloc(&abase, cap) == cudaSuccess) {
             arena.base = static_cast<char *>(abase);
-            arena.cap = budget;
+            arena.cap = cap;
         } else {
             cudaGetLastError();
         }

@@ -72,6 +72,7 @@ struct Bufs {
     // use_seeds is set the TMA-fed scorer takes its starting bounds from them
     const int *seeds;
     const float *seed_d;
+    float *bound;  // forward: [p][n_rows] starting bounds of a seeded step (k_seed_bounds)
     int use_seeds;
 };
 
@@ -96,6 +97,8 @@ void clear_error();
 // Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 64.
 bool score_tma_supported(int kmax);  // kernel option 3: k_max <= 64
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
+// Seeded forward steps: each candidate's starting bound from the seed columns, into b.bound.
+cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s);
 
 // Commit the winner into D (snn_commit.cu); forward commits given seed
 // buffers also keep kSeeds near columns per row for the next step's bounds.

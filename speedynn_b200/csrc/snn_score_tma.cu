@@ -22,7 +22,8 @@
 //     at or below it): a first pass over a quarter of the columns (per-lane
 //     minima, their k-th smallest); or, on seeded forward steps, the k-th
 //     smallest exact distance over the row's 128 seed columns (the columns
-//     nearest the row under the committed D, kept by the last commit); or, on
+//     nearest the row under the committed D, kept by the last commit),
+//     computed beforehand by k_seed_bounds; or, on
 //     backward steps after the first, the previous step's k-th distances
 //     (kth_prev), which removal only lowers.
 //   * Full pass: a conservative sign-bit filter (one sub and one FMA per
@@ -371,32 +372,63 @@ __device__ __forceinline__ float warp_kth(float (&v)[V], int K, int lane)
     return __shfl_sync(kFull, sel, (K - 1) / V);
 }
 
-// Starting bound of one forward problem from the scored row's kSeeds seed
-// columns (snn_commit.cu): the K-th smallest exact distance
-// d = fl(D + fl((x - x_i)^2)) over them.  Any K distinct columns have their
-// K-th smallest distance at or above the final K-th neighbour distance, so it
-// is an inclusive bound; padding seeds (index -1) and NaN distances count as
-// +inf.  sd[j], si[j]: the row's seeds j*32 + lane; xc: the candidate's
-// training values.  For K <= 32 the K-th of the 64 values made of each lane's
-// two smallest is taken (a subset: still K distinct columns, and as tight as
-// all 128 unless a lane holds three of the K nearest).
-template <int KL>
-__device__ __forceinline__ float seed_bound(const float (&sd)[4], const int (&si)[4], float x, const float *xc, int K,
-                                            int lane)
+// k_seed_bounds: the starting bound of every (candidate, scored row) problem
+// of a seeded forward step, bound[c][r] = the K-th smallest exact distance
+// d = fl(D + fl((x_r,c - x_i,c)^2)) over the row's kSeeds seed columns (kept
+// by the last commit, snn_commit.cu).  Any K distinct columns have their K-th
+// smallest distance at or above the final K-th neighbour distance, so it is an
+// inclusive bound; padding seeds (index -1) and NaN distances count as +inf.
+// One warp per row, lane l holding seeds l, l+32, l+64, l+96; the gathers of
+// four candidates are issued together, and many warps per SM hide their
+// latency.  For K <= 32 the K-th of the 64 values made of each lane's two
+// smallest is taken (a subset: still K distinct columns, and as tight as all
+// 128 unless a lane holds three of the K nearest); for K <= 64 all 128.
+template <int V>
+__global__ void __launch_bounds__(256) k_seed_bounds(Bufs b, int n_cand, float *bound)
 {
-    float v[4];
+    if (b.st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (r >= b.n_rows) return;
+    const int K = b.kmax;
+    int si[4];
+    float sd[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const float d = si[j] >= 0 ? __fadd_rn(sd[j], sqdiff1(x, __ldg(xc + si[j]))) : INFINITY;
-        v[j] = d <= FLT_MAX ? d : INFINITY;
+        si[j] = __ldg(b.seeds + (size_t)r * kSeeds + j * 32 + lane);
+        sd[j] = __ldg(b.seed_d + (size_t)r * kSeeds + j * 32 + lane);
     }
-    if constexpr (KL > 32) {
-        return warp_kth<4>(v, K, lane);
-    } else {
-        const float a = fminf(v[0], v[1]), b = fmaxf(v[0], v[1]);
-        const float c = fminf(v[2], v[3]), e = fmaxf(v[2], v[3]);
-        float two[2] = {fminf(a, c), fminf(fmaxf(a, c), fminf(b, e))};
-        return warp_kth<2>(two, K, lane);
+    for (int c0 = 0; c0 < n_cand; c0 += 4) {
+        int cid[4];
+        float xr[4], g[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            cid[q] = c0 + q < n_cand ? __ldg(b.cands + c0 + q) : -1;
+            xr[q] = cid[q] >= 0 ? __ldg(b.XV + (size_t)cid[q] * b.ldr + r) : 0.0f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                g[q][j] = cid[q] >= 0 && si[j] >= 0 ? __ldg(b.XT + (size_t)cid[q] * b.ldc + si[j]) : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (cid[q] < 0) break;  // warp-uniform
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float d = si[j] >= 0 ? __fadd_rn(sd[j], sqdiff1(xr[q], g[q][j])) : INFINITY;
+                v[j] = d <= FLT_MAX ? d : INFINITY;
+            }
+            float T;
+            if constexpr (V == 4) {
+                T = warp_kth<4>(v, K, lane);
+            } else {
+                const float a = fminf(v[0], v[1]), bb = fmaxf(v[0], v[1]);
+                const float c = fminf(v[2], v[3]), e = fmaxf(v[2], v[3]);
+                float two[2] = {fminf(a, c), fminf(fmaxf(a, c), fminf(bb, e))};
+                T = warp_kth<2>(two, K, lane);
+            }
+            if (lane == 0) bound[(size_t)cid[q] * b.n_rows + r] = T;
+        }
     }
 }
 
@@ -468,7 +500,7 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int
     const bool reuse = BWD && b.use_prev && b.kth_prev != nullptr;
     // Seeded forward steps take their bounds from the previous commit's seed
     // columns and skip the first pass as well.
-    const bool seeded = !BWD && b.use_seeds && b.seeds != nullptr && b.seed_d != nullptr;
+    const bool seeded = !BWD && b.use_seeds && b.bound != nullptr;
     const int nA = reuse || seeded ? 0 : (nstages >= 4 ? nstages / 4 : 1);
     const int nvirt = nA + nstages;
 
@@ -565,28 +597,15 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int
     // For k_max > 32 each lane keeps two minima (its even and its odd columns),
     // 64 values from distinct columns.
     if (seeded) {
-        // One problem at a time (warp-uniform): gather the candidate's values at
-        // the row's seed columns, exact distances, K-th smallest.
-#pragma unroll 1
-        for (int ri = 0; ri < kRW; ++ri) {
-            const int r = wr0 + ri;
-            float sd[4];
-            int si[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                si[j] = r < b.n_rows ? __ldg(b.seeds + (size_t)r * kSeeds + j * 32 + lane) : -1;
-                sd[j] = r < b.n_rows ? __ldg(b.seed_d + (size_t)r * kSeeds + j * 32 + lane) : INFINITY;
+        // bounds from the seed columns, computed by k_seed_bounds
+        if (lane < kP) {
+            const int p = lane;
+            float th = -1.0f;  // padded problem: never passes
+            if ((okmask >> p) & 1u) {
+                const float T = b.bound[(size_t)S.srcand[wc + p % kCW] * b.n_rows + wr0 + p / kCW];
+                th = T < FLT_MAX ? T : 0x1.fffffcp+127f;  // inclusive; FLT_MAX itself never enters
             }
-#pragma unroll 1
-            for (int ci = 0; ci < kCW; ++ci) {
-                const int p = ri * kCW + ci;
-                float th = -1.0f;  // padded problem: never passes
-                if ((okmask >> p) & 1u) {
-                    const float T = seed_bound<KL>(sd, si, myX[p], b.XT + (size_t)S.srcand[wc + ci] * b.ldc, K, lane);
-                    th = T < FLT_MAX ? T : 0x1.fffffcp+127f;  // inclusive; FLT_MAX itself never enters
-                }
-                if (lane == 0) myT[p] = th;
-            }
+            myT[p] = th;
         }
         __syncwarp();
     } else {
@@ -902,6 +921,14 @@ cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 }
 
 }  // namespace
+
+cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s)
+{
+    const int grid = (b.n_rows + 7) / 8;
+    if (list_slots(b.kmax) > 32) k_seed_bounds<4><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
+    else k_seed_bounds<2><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s)
 {
