@@ -422,8 +422,9 @@ def run_ours(args, world, rank, local):
     clk = Clocks(gpu_index)
     barrier()
     clk.start()
-    tot_ms = score_ms = commit_ms = 0.0
+    tot_ms = score_ms = commit_ms = setup_ms = 0.0
     score_n = commit_n = launches = 0
+    step_score = np.zeros(steps)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sel.run()
@@ -434,6 +435,8 @@ def run_ours(args, world, rank, local):
         commit_ms += tm["commit_ms"]
         commit_n += tm["commit_launches"]
         launches += tm["launches"]
+        setup_ms += sel.setup_ms()
+        step_score += sel.step_timing()[0][:steps]
     barrier()
     wall = time.perf_counter() - t0
     clocks = clk.stop()
@@ -489,7 +492,9 @@ def run_ours(args, world, rank, local):
             "config": dict(workload_desc(k, steps, n_train, n_val, p, name), parallelism=f"independent problems x{world}"),
             "greedy_step_ms": ms_step / steps,
             "breakdown_ms_per_step": {"score": score_ms / args.steps, "commit": commit_ms / args.steps,
-                                      "other": (tot_ms - score_ms - commit_ms) / args.steps},
+                                      "initial_distance": setup_ms / args.steps,
+                                      "other": (tot_ms - score_ms - commit_ms - setup_ms) / args.steps},
+            "score_ms_per_greedy_step": [round(float(x) / args.steps, 3) for x in step_score],
             "wall_ms_per_step": 1000.0 * wall / args.steps,
             "e2e": None if args.no_e2e else {"value": world * evals / e2e_s, "unit": UNIT,
                                              "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

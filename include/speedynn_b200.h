@@ -225,6 +225,13 @@ SNN_API int snn_get_filter_counters(snn_handle *h, unsigned long long *row_chunk
  * number of steps timed. */
 SNN_API int snn_get_step_timing(snn_handle *h, float *score_ms, float *commit_ms, int n);
 
+/* CUDA-event milliseconds of the last reset's initial distance matrix: the
+ * full distance over all features for backward elimination
+ * (compute_distance_matrix_cpu, speedynn/lib/cpu.c:185-215, plus the per-row
+ * maxima of the backward filter), the empty matrix for forward selection
+ * (empty_distance_matrix_cpu, cpu.c:171-183).  Every run starts with a reset. */
+SNN_API int snn_get_setup_timing(snn_handle *h, float *ms);
+
 SNN_API int snn_destroy(snn_handle *h);
 
 /* ---------------------------------------------------------------------------

@@ -82,6 +82,7 @@ def lib():
                                                        ctypes.POINTER(ctypes.c_ulonglong),
                                                        ctypes.POINTER(ctypes.c_ulonglong)]),
             "snn_get_step_timing": (ctypes.c_int, [vp, _f32p, _f32p, ctypes.c_int]),
+            "snn_get_setup_timing": (ctypes.c_int, [vp, _f32p]),
             "snn_batch_create": (ctypes.c_int, [ctypes.POINTER(SnnDesc), ctypes.c_int, ctypes.c_ulonglong,
                                                 ctypes.POINTER(vp)]),
             "snn_batch_load": (ctypes.c_int, [vp, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]),

@@ -115,6 +115,8 @@ struct snn_handle {
     bool arena = false;       // device buffers are sub-allocations of a batch arena (never freed one by one)
     std::vector<EventPair> score_ev, commit_ev;
     EventPair total_ev;
+    EventPair setup_ev;  // the last reset's initial distance matrix (full distance or empty)
+    bool setup_timed = false;
     int n_score = 0, n_commit = 0, n_launch = 0;
 
     Bufs bufs() const
@@ -230,6 +232,8 @@ void free_all(snn_handle *h)
     }
     if (h->total_ev.a) cudaEventDestroy(h->total_ev.a);
     if (h->total_ev.b) cudaEventDestroy(h->total_ev.b);
+    if (h->setup_ev.a) cudaEventDestroy(h->setup_ev.a);
+    if (h->setup_ev.b) cudaEventDestroy(h->setup_ev.b);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -350,6 +354,11 @@ int issue_reset(snn_handle *h)
     h->last_ncand = 0;
     const Bufs b = h->bufs();
     SNN_CUDA(snn::launch_reset_state(b, h->desc.backward, h->total_steps, h->stream));
+    h->setup_timed = h->step_events;
+    if (h->setup_timed) {
+        if (int rc = make_pair(h->setup_ev)) return rc;
+        SNN_CUDA(cudaEventRecord(h->setup_ev.a, h->stream));
+    }
     if (h->desc.backward) {
         SNN_CUDA(snn::launch_full_distance(b, h->cv, h->npf, h->stream));
         SNN_CUDA(snn::launch_row_dmax(b, h->dmax, h->stream));
@@ -357,6 +366,7 @@ int issue_reset(snn_handle *h)
     } else {
         SNN_CUDA(snn::launch_init_forward(b, h->cv, h->npf, h->stream));
     }
+    if (h->setup_timed) SNN_CUDA(cudaEventRecord(h->setup_ev.b, h->stream));
     h->n_launch += 2;
     h->host_step = 0;
     return SNN_OK;
@@ -922,6 +932,17 @@ SNN_API int snn_get_step_timing(snn_handle *h, float *score_ms, float *commit_ms
         }
     }
     return h->n_score;
+}
+
+SNN_API int snn_get_setup_timing(snn_handle *h, float *ms)
+{
+    g_err.clear();
+    if (!h || !ms) return fail(SNN_ERR_ARG, "null handle or output");
+    if (!h->setup_timed) return fail(SNN_ERR_STATE, "no timed reset (the handle was never loaded or reset)");
+    SNN_CUDA(cudaSetDevice(h->device));
+    SNN_CUDA(cudaStreamSynchronize(h->stream));
+    SNN_CUDA(cudaEventElapsedTime(ms, h->setup_ev.a, h->setup_ev.b));
+    return SNN_OK;
 }
 
 SNN_API int snn_destroy(snn_handle *h)

@@ -171,6 +171,12 @@ class Selector:
         k = check(_lib.lib().snn_get_step_timing(self._h, ptr(sc, _f32p), ptr(cm, _f32p), n))
         return sc[:k], cm[:k]
 
+    def setup_ms(self):
+        """CUDA-event time of the last reset's initial distance matrix (backward: the full distance)."""
+        ms = ctypes.c_float()
+        check(_lib.lib().snn_get_setup_timing(self._h, ctypes.byref(ms)))
+        return ms.value
+
     def timing(self):
         s, c, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         ns, nc, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
