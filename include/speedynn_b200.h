@@ -204,10 +204,10 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
 #define SNN_OPT_COUNTERS 3
 /*   SNN_OPT_SEED_STEP forward step (= features already committed) from which
  *                  the TMA-fed scorer takes each candidate's starting bound on
- *                  its k-th neighbour distance from 128 "seed" columns near
+ *                  its k-th neighbour distance from 256 "seed" columns near
  *                  the row (kept by the previous commit) instead of a first
  *                  pass over a quarter of the columns.  Results are identical;
- *                  only the work differs.  Default 4; a large value turns it
+ *                  only the work differs.  Default 2; a large value turns it
  *                  off. */
 #define SNN_OPT_SEED_STEP 4
 SNN_API int snn_set_option(snn_handle *h, int option, int value);

@@ -98,7 +98,7 @@ struct snn_handle {
     float *seed_d = nullptr;
     float *sbound = nullptr;      // [p][n_rows] starting bounds of a seeded step
     bool seeds_ok = false;        // seeds hold the current D's seed columns
-    int seed_step = 4;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds
+    int seed_step = 2;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds
     unsigned long long *fcount = nullptr;  // filter counters of the TMA-fed scorer (3)
     bool count_filter = false;             // SNN_OPT_COUNTERS
     int kernel = 0;               // scoring kernel: 0 auto, 1 rows per lane, 3 TMA-fed row tiles
@@ -265,11 +265,12 @@ int check_device(int device)
 bool use_tma(const snn_handle *h) { return h->kernel == 3 || (h->kernel == 0 && snn::score_tma_supported(h->kmax)); }
 
 // Forward step t (t features committed) is scored from seed bounds once
-// t >= seed_step: after a few commits the columns nearest under D are near
-// under D + one more feature too, and the seed bound beats a first pass over a
-// quarter of the columns (measured on the fwd-64k data: ~13 list entries per
-// problem against ~47 at step 14, about the same at step 4).  The commit
-// before such a step writes the seeds.
+// t >= seed_step: after two commits the columns nearest under D are mostly
+// near under D + one more feature too, and the bound over 256 of them beats a
+// first pass over a quarter of the columns (on the fwd-64k data, rows whose
+// filter fires: 17.9 % against 21.5 % at step 2, 6.9 % against 12.1 % at
+// step 14; at step 1, with one feature committed, the first pass is better).
+// The commit before such a step writes the seeds.
 bool seeds_for_step(const snn_handle *h, int t)
 {
     return !h->desc.backward && h->seeds && use_tma(h) && t >= h->seed_step;

@@ -8,15 +8,15 @@
 // stores (HBM-bound: 8 bytes per entry).
 //
 // Seeds (forward steps only).  While it streams a row, each lane also keeps
-// the four smallest new distances among the columns it visits (lane l sees
-// the float4 groups l, l+32, l+64, ...), so every row leaves 128 distinct
-// real columns that lie near it under the committed features: seeds[r][j*32+l]
-// and their distances seed_d[r][j*32+l] (lane l's j-th smallest; index -1 and
-// +inf where a lane saw fewer than four finite distances).  The next forward
-// scoring launch takes, for each candidate, the k-th smallest exact distance
-// over these columns as its starting bound on the candidate's k-th neighbour
-// distance (any k distinct columns bound it; near ones bound it tightly), in
-// place of a first pass over the columns.
+// the kSeedsPerLane (8) smallest new distances among the columns it visits
+// (lane l sees the float4 groups l, l+32, l+64, ...), so every row leaves 256
+// distinct real columns that lie near it under the committed features:
+// seeds[r][j*32+l] and their distances seed_d[r][j*32+l] (lane l's j-th
+// smallest; index -1 and +inf where a lane saw fewer finite distances).  The
+// next forward scoring step takes, for each candidate, the k-th smallest
+// exact distance over these columns as its starting bound on the candidate's
+// k-th neighbour distance (any k distinct columns bound it; near ones bound it
+// tightly), in place of a first pass over the columns (k_seed_bounds).
 #include <float.h>
 #include <math.h>
 
@@ -32,33 +32,30 @@ __device__ __forceinline__ float sqdiff(float a, float b)
     return __fmul_rn(t, t);
 }
 
-// Insert (v, col) into the lane's ascending four-entry list if v is below its
-// last entry (strict: +inf and NaN never enter).
-__device__ __forceinline__ void keep4(float (&s)[4], int (&i)[4], float v, int col)
+// Insert (v, col) into the lane's ascending N-entry list if v is below its
+// last entry (strict: +inf and NaN never enter).  Fully unrolled, so the list
+// stays in registers.
+template <int N>
+__device__ __forceinline__ void keep_n(float (&s)[N], int (&i)[N], float v, int col)
 {
-    if (!(v < s[3])) return;
-    if (v < s[2]) {
-        s[3] = s[2];
-        i[3] = i[2];
-        if (v < s[1]) {
-            s[2] = s[1];
-            i[2] = i[1];
-            if (v < s[0]) {
-                s[1] = s[0];
-                i[1] = i[0];
-                s[0] = v;
-                i[0] = col;
+    if (!(v < s[N - 1])) return;
+    bool placed = false;
+#pragma unroll
+    for (int j = N - 1; j > 0; --j) {
+        if (!placed) {
+            if (v < s[j - 1]) {
+                s[j] = s[j - 1];
+                i[j] = i[j - 1];
             } else {
-                s[1] = v;
-                i[1] = col;
+                s[j] = v;
+                i[j] = col;
+                placed = true;
             }
-        } else {
-            s[2] = v;
-            i[2] = col;
         }
-    } else {
-        s[3] = v;
-        i[3] = col;
+    }
+    if (!placed) {
+        s[0] = v;
+        i[0] = col;
     }
 }
 
@@ -76,8 +73,13 @@ __global__ void __launch_bounds__(256) k_commit(Bufs b, int *seeds, float *seed_
     for (int r = blockIdx.x * wpb + (threadIdx.x >> 5); r < b.n_rows; r += gridDim.x * wpb) {
         const float a = __ldg(xv + r);
         float4 *row = reinterpret_cast<float4 *>(b.D + (size_t)r * b.ldc);
-        float sv[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-        int si[4] = {-1, -1, -1, -1};
+        float sv[kSeedsPerLane];
+        int si[kSeedsPerLane];
+#pragma unroll
+        for (int j = 0; j < kSeedsPerLane; ++j) {
+            sv[j] = INFINITY;
+            si[j] = -1;
+        }
         for (int q0 = 0; q0 < n4; q0 += 128) {  // 4 float4 per lane in flight
             float4 d[4], c[4];
 #pragma unroll
@@ -105,17 +107,17 @@ __global__ void __launch_bounds__(256) k_commit(Bufs b, int *seeds, float *seed_
                     }
                     __stcs(row + q, d[u]);
                     if (SEEDS) {
-                        keep4(sv, si, d[u].x, 4 * q);
-                        keep4(sv, si, d[u].y, 4 * q + 1);
-                        keep4(sv, si, d[u].z, 4 * q + 2);
-                        keep4(sv, si, d[u].w, 4 * q + 3);
+                        keep_n(sv, si, d[u].x, 4 * q);
+                        keep_n(sv, si, d[u].y, 4 * q + 1);
+                        keep_n(sv, si, d[u].z, 4 * q + 2);
+                        keep_n(sv, si, d[u].w, 4 * q + 3);
                     }
                 }
             }
         }
         if (SEEDS) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < kSeedsPerLane; ++j) {
                 seeds[(size_t)r * kSeeds + j * 32 + lane] = si[j];
                 seed_d[(size_t)r * kSeeds + j * 32 + lane] = sv[j];
             }

@@ -102,7 +102,8 @@ cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s);
 
 // Commit the winner into D (snn_commit.cu); forward commits given seed
 // buffers also keep kSeeds near columns per row for the next step's bounds.
-constexpr int kSeeds = 128;  // seed columns per row: four per lane of a warp
+constexpr int kSeedsPerLane = 8;        // seed columns each lane of the commit keeps
+constexpr int kSeeds = 32 * kSeedsPerLane;  // seed columns per row
 cudaError_t launch_commit(const Bufs &b, int backward, int *seeds, float *seed_d, cudaStream_t s);
 
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);

@@ -21,7 +21,7 @@
 //   * Starting bound on each problem's k-th distance (k distinct columns lie
 //     at or below it): a first pass over a quarter of the columns (per-lane
 //     minima, their k-th smallest); or, on seeded forward steps, the k-th
-//     smallest exact distance over the row's 128 seed columns (the columns
+//     smallest exact distance over the row's 256 seed columns (the columns
 //     nearest the row under the committed D, kept by the last commit),
 //     computed beforehand by k_seed_bounds; or, on
 //     backward steps after the first, the previous step's k-th distances
@@ -374,59 +374,63 @@ __device__ __forceinline__ float warp_kth(float (&v)[V], int K, int lane)
 
 // k_seed_bounds: the starting bound of every (candidate, scored row) problem
 // of a seeded forward step, bound[c][r] = the K-th smallest exact distance
-// d = fl(D + fl((x_r,c - x_i,c)^2)) over the row's kSeeds seed columns (kept
-// by the last commit, snn_commit.cu).  Any K distinct columns have their K-th
-// smallest distance at or above the final K-th neighbour distance, so it is an
-// inclusive bound; padding seeds (index -1) and NaN distances count as +inf.
-// One warp per row, lane l holding seeds l, l+32, l+64, l+96; the gathers of
-// four candidates are issued together, and many warps per SM hide their
-// latency.  For K <= 32 the K-th of the 64 values made of each lane's two
-// smallest is taken (a subset: still K distinct columns, and as tight as all
-// 128 unless a lane holds three of the K nearest); for K <= 64 all 128.
+// d = fl(D + fl((x_r,c - x_i,c)^2)) over columns of the row's kSeeds seed
+// columns (kept by the last commit, snn_commit.cu).  Any K distinct columns
+// have their K-th smallest distance at or above the final K-th neighbour
+// distance, so it is an inclusive bound; padding seeds (index -1) and NaN
+// distances count as +inf.  One warp per row, lane l holding seeds
+// l + 32 j (j < kSeedsPerLane); the gathers of two candidates are issued
+// together, and many warps per SM hide their latency.  Each lane keeps its
+// V smallest values (V = 2 for K <= 16, 4 above), and the K-th smallest of
+// those 32 V values is the bound: a subset of the seeds, so still K distinct
+// columns, and as tight as all of them unless a lane holds more than V of
+// the K nearest.
 template <int V>
 __global__ void __launch_bounds__(256) k_seed_bounds(Bufs b, int n_cand, float *bound)
 {
+    constexpr int S = kSeedsPerLane;
     if (b.st->done) return;
     const int lane = threadIdx.x & 31;
     const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (r >= b.n_rows) return;
     const int K = b.kmax;
-    int si[4];
-    float sd[4];
+    int si[S];
+    float sd[S];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < S; ++j) {
         si[j] = __ldg(b.seeds + (size_t)r * kSeeds + j * 32 + lane);
         sd[j] = __ldg(b.seed_d + (size_t)r * kSeeds + j * 32 + lane);
     }
-    for (int c0 = 0; c0 < n_cand; c0 += 4) {
-        int cid[4];
-        float xr[4], g[4][4];
+    for (int c0 = 0; c0 < n_cand; c0 += 2) {
+        int cid[2];
+        float xr[2], g[2][S];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
             cid[q] = c0 + q < n_cand ? __ldg(b.cands + c0 + q) : -1;
             xr[q] = cid[q] >= 0 ? __ldg(b.XV + (size_t)cid[q] * b.ldr + r) : 0.0f;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < S; ++j)
                 g[q][j] = cid[q] >= 0 && si[j] >= 0 ? __ldg(b.XT + (size_t)cid[q] * b.ldc + si[j]) : 0.0f;
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
             if (cid[q] < 0) break;  // warp-uniform
-            float v[4];
+            // the lane's V smallest of its S distances, by insertion into a sorted list
+            float best[V];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float d = si[j] >= 0 ? __fadd_rn(sd[j], sqdiff1(xr[q], g[q][j])) : INFINITY;
-                v[j] = d <= FLT_MAX ? d : INFINITY;
+            for (int h = 0; h < V; ++h) best[h] = INFINITY;
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                float d = si[j] >= 0 ? __fadd_rn(sd[j], sqdiff1(xr[q], g[q][j])) : INFINITY;
+                d = d <= FLT_MAX ? d : INFINITY;
+#pragma unroll
+                for (int h = 0; h < V; ++h) {  // compare-exchange down the list
+                    const float lo = fminf(best[h], d);
+                    d = fmaxf(best[h], d);
+                    best[h] = lo;
+                }
             }
-            float T;
-            if constexpr (V == 4) {
-                T = warp_kth<4>(v, K, lane);
-            } else {
-                const float a = fminf(v[0], v[1]), bb = fmaxf(v[0], v[1]);
-                const float c = fminf(v[2], v[3]), e = fmaxf(v[2], v[3]);
-                float two[2] = {fminf(a, c), fminf(fmaxf(a, c), fminf(bb, e))};
-                T = warp_kth<2>(two, K, lane);
-            }
+            const float T = warp_kth<V>(best, K, lane);
             if (lane == 0) bound[(size_t)cid[q] * b.n_rows + r] = T;
         }
     }
@@ -925,7 +929,7 @@ cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s)
 {
     const int grid = (b.n_rows + 7) / 8;
-    if (list_slots(b.kmax) > 32) k_seed_bounds<4><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
+    if (b.kmax > 16) k_seed_bounds<4><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
     else k_seed_bounds<2><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
     return cudaGetLastError();
 }
