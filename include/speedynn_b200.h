@@ -207,8 +207,8 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
  *                  its k-th neighbour distance from 256 "seed" columns near
  *                  the row (kept by the previous commit) instead of a first
  *                  pass over a quarter of the columns.  Results are identical;
- *                  only the work differs.  Default 2; a large value turns it
- *                  off. */
+ *                  only the work differs.  Default 2 (3 when k_max > 16); a
+ *                  large value turns it off. */
 #define SNN_OPT_SEED_STEP 4
 SNN_API int snn_set_option(snn_handle *h, int option, int value);
 

@@ -98,7 +98,7 @@ struct snn_handle {
     float *seed_d = nullptr;
     float *sbound = nullptr;      // [p][n_rows] starting bounds of a seeded step
     bool seeds_ok = false;        // seeds hold the current D's seed columns
-    int seed_step = 2;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds
+    int seed_step = 2;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds (set at create)
     unsigned long long *fcount = nullptr;  // filter counters of the TMA-fed scorer (3)
     bool count_filter = false;             // SNN_OPT_COUNTERS
     int kernel = 0;               // scoring kernel: 0 auto, 1 rows per lane, 3 TMA-fed row tiles
@@ -270,7 +270,10 @@ bool use_tma(const snn_handle *h) { return h->kernel == 3 || (h->kernel == 0 && 
 // first pass over a quarter of the columns (on the fwd-64k data, rows whose
 // filter fires: 17.9 % against 21.5 % at step 2, 6.9 % against 12.1 % at
 // step 14; at step 1, with one feature committed, the first pass is better).
-// The commit before such a step writes the seeds.
+// With k above 16 the seeds start a step later: a k-th distance over the
+// seeds needs them to be near in more features (fwd-200k, k = 50: step 2
+// took 913 ms seeded against 845 ms with the first pass, step 3 767 against
+// 825).  The commit before such a step writes the seeds.
 bool seeds_for_step(const snn_handle *h, int t)
 {
     return !h->desc.backward && h->seeds && use_tma(h) && t >= h->seed_step;
@@ -463,6 +466,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     h->n_rows = cv ? d->n_train : d->n_val;
     h->npf = cv ? d->n_train / d->k_fold : 1;
     h->kmax = kmax;
+    h->seed_step = kmax <= 16 ? 2 : 3;
     h->nk = d->num_k_vals;
     h->ldc = round_up(h->n_cols, snn::kPadCols);
     h->ldr = cv ? h->ldc : round_up(h->n_rows, snn::kPadCols);

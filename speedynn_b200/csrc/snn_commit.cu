@@ -59,8 +59,10 @@ __device__ __forceinline__ void keep_n(float (&s)[N], int (&i)[N], float v, int 
     }
 }
 
+// At most 64 registers (4 blocks of 256 threads per SM): the stream needs
+// the warps to keep enough loads in flight to stay HBM-bound.
 template <bool BWD, bool SEEDS>
-__global__ void __launch_bounds__(256) k_commit(Bufs b, int *seeds, float *seed_d)
+__global__ void __launch_bounds__(256, 4) k_commit(Bufs b, int *seeds, float *seed_d)
 {
     if (b.st->done) return;
     const int lane = threadIdx.x & 31;
@@ -80,10 +82,12 @@ __global__ void __launch_bounds__(256) k_commit(Bufs b, int *seeds, float *seed_
             sv[j] = INFINITY;
             si[j] = -1;
         }
-        for (int q0 = 0; q0 < n4; q0 += 128) {  // 4 float4 per lane in flight
-            float4 d[4], c[4];
+        // U float4 per lane in flight (2 when the seed lists take registers)
+        constexpr int U = SEEDS ? 2 : 4;
+        for (int q0 = 0; q0 < n4; q0 += 32 * U) {
+            float4 d[U], c[U];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const int q = q0 + u * 32 + lane;
                 if (q < n4) {
                     d[u] = __ldcs(row + q);
@@ -91,7 +95,7 @@ __global__ void __launch_bounds__(256) k_commit(Bufs b, int *seeds, float *seed_
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const int q = q0 + u * 32 + lane;
                 if (q < n4) {
                     if (BWD) {

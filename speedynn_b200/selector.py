@@ -149,7 +149,7 @@ class Selector:
         check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_KERNEL, int(which)))
 
     def set_seed_step(self, step):
-        """First forward step whose starting bounds come from seed columns (default 2;
+        """First forward step whose starting bounds come from seed columns (default 2, 3 for k > 16;
         a large value turns seeded steps off).  Results do not depend on it."""
         check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_SEED_STEP, int(step)))
 
