@@ -23,6 +23,7 @@ SNN_ERR_TIMEOUT = -7
 SNN_OPT_KERNEL = 2
 SNN_OPT_COUNTERS = 3
 SNN_OPT_SEED_STEP = 4
+SNN_OPT_SORTED_START = 5
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f32p = ctypes.POINTER(ctypes.c_float)

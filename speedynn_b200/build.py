@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspeedynn_b200.so")
-SOURCES = ["snn_kernels.cu", "snn_score.cu", "snn_commit.cu", "snn_score_tma.cu", "snn_model.cu", "snn_noalloc.cu", "snn_api.cu", "snn_compat.cpp"]
+SOURCES = ["snn_kernels.cu", "snn_score.cu", "snn_commit.cu", "snn_sorted.cu", "snn_score_tma.cu", "snn_model.cu", "snn_noalloc.cu", "snn_api.cu", "snn_compat.cpp"]
 HEADERS = ["snn_internal.h"]
 
 NVCC_FLAGS = [

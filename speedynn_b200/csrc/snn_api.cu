@@ -97,6 +97,13 @@ struct snn_handle {
     int *seeds = nullptr;
     float *seed_d = nullptr;
     float *sbound = nullptr;      // [p][n_rows] starting bounds of a seeded step
+    // forward holdout: training values of each feature sorted ([p][ldc], with
+    // their column indices) for the first step, and the sort's work buffers
+    float *sval = nullptr, *skey = nullptr;
+    int *sidx = nullptr, *sord = nullptr, *soff = nullptr;
+    char *stemp = nullptr;
+    size_t stemp_bytes = 0;
+    bool sorted_start = true;     // SNN_OPT_SORTED_START
     bool seeds_ok = false;        // seeds hold the current D's seed columns
     int seed_step = 2;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds (set at create)
     unsigned long long *fcount = nullptr;  // filter counters of the TMA-fed scorer (3)
@@ -163,6 +170,7 @@ struct snn_handle {
         b.seed_d = seed_d;
         b.bound = sbound;
         b.use_seeds = 0;
+        b.only_if_full = 0;
         return b;
     }
 };
@@ -217,7 +225,8 @@ void free_all(snn_handle *h)
     if (!h->arena) {  // an arena's buffers are freed by its owner
         void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                         h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
-                        h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->sbound, h->perm, h->fvar,
+                        h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->sbound, h->sval, h->skey, h->sidx,
+                        h->sord, h->soff, h->stemp, h->perm, h->fvar,
                         h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
         for (void *q : ptrs)
             if (q) cudaFree(q);
@@ -279,6 +288,10 @@ bool seeds_for_step(const snn_handle *h, int t)
     return !h->desc.backward && h->seeds && use_tma(h) && t >= h->seed_step;
 }
 
+// The first forward step of a holdout problem runs from sorted feature columns
+// (D is still zero there); CV mode excludes same-fold pairs and takes the scan.
+bool sorted_step(const snn_handle *h, int t) { return t == 0 && h->sorted_start && h->sval && !h->desc.backward && !h->cv; }
+
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)
 {
@@ -298,6 +311,11 @@ int issue_step(snn_handle *h, int t)
         return fail(SNN_ERR_CUDA, "injected launch failure at step %d", t);
     }
     bool tma_step = false;
+    if (sorted_step(h, t)) {
+        SNN_CUDA(snn::launch_first_step(b, h->sval, h->sidx, n_cand, h->stream));
+        b.only_if_full = 1;  // the scan below runs only if some tie group was too large
+        h->n_launch += 1;
+    }
     if (use_tma(h)) {
         b.use_prev = backward && h->prev_ok ? 1 : 0;
         b.use_seeds = seeds_for_step(h, t) && h->seeds_ok ? 1 : 0;
@@ -434,6 +452,8 @@ static size_t handle_bytes(const snn_desc *d, int kmax)
     (void)kmax;
     size_t f = p * ldc + n_rows * ldc + p * (size_t)d->num_k_vals * n_rows + std::max(n_rows, n_cols) * p +
                n_rows * M + n_cols + n_rows;
+    // sorted feature columns of the first forward step and the sort's buffers
+    if (!d->backward && !cv) f += 4 * p * ldc + 2 * p + snn::sort_temp_bytes(d->p, (int)ldc) / sizeof(float) + 1;
     if (d->backward) f += p * n_rows + n_rows;  // kth_prev, dmax
     if (!cv) f += p * ldr;
     return sizeof(float) * f + ((size_t)1 << 20);
@@ -525,6 +545,16 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
         if ((rc = dev_alloc(&h->seed_d, (size_t)h->n_rows * snn::kSeeds, "seed distances"))) return bail(rc);
         if ((rc = dev_alloc(&h->sbound, p * h->n_rows, "seed bounds"))) return bail(rc);
     }
+    if (!d->backward && !cv) {
+        const size_t pl = p * h->ldc;
+        if ((rc = dev_alloc(&h->sval, pl, "sorted values"))) return bail(rc);
+        if ((rc = dev_alloc(&h->skey, pl, "sort keys"))) return bail(rc);
+        if ((rc = dev_alloc(&h->sidx, pl, "sorted indices"))) return bail(rc);
+        if ((rc = dev_alloc(&h->sord, pl, "sort values"))) return bail(rc);
+        if ((rc = dev_alloc(&h->soff, 2 * p, "sort offsets"))) return bail(rc);
+        h->stemp_bytes = snn::sort_temp_bytes(h->p, h->ldc);
+        if ((rc = dev_alloc(&h->stemp, h->stemp_bytes, "sort workspace"))) return bail(rc);
+    }
     // On the handle's stream, so every kernel that reads k_vals comes after it
     // (the source lives as long as the handle).  A cudaMemcpy here would run on
     // the legacy stream, which does not order the handle's non-blocking stream,
@@ -574,6 +604,9 @@ static int load_impl(snn_handle *h, const float *X_train, const float *y_train, 
     // similar scale (any order gives the same results)
     SNN_CUDA(snn::launch_feature_variance(h->bufs(), h->fvar, h->stream));
     SNN_CUDA(snn::launch_feature_order(h->fvar, h->p, h->perm, h->stream));
+    if (h->sval)
+        SNN_CUDA(snn::launch_sort_features(h->bufs(), h->skey, h->sord, h->soff, h->sval, h->sidx, h->stemp,
+                                           h->stemp_bytes, h->stream));
     h->loaded = true;
     reset_timing(h);
     if (int rc = issue_reset(h)) return rc;
@@ -893,6 +926,7 @@ SNN_API int snn_set_option(snn_handle *h, int option, int value)
         h->kernel = value;
         h->seeds_ok = false;
         return SNN_OK;
+    case SNN_OPT_SORTED_START: h->sorted_start = value != 0; return SNN_OK;
     case SNN_OPT_SEED_STEP:
         if (value < 1) return fail(SNN_ERR_ARG, "seed step %d must be >= 1", value);
         h->seed_step = value;

@@ -18,7 +18,7 @@ struct State {
     int n_cand;       // candidates of the next step
     int best_k_last;  // best k of the last winner
     int num_final;    // features in the model after the last step
-    int pad;
+    int full_scan;    // 1: the sorted first step left problems to the full scan (snn_sorted.cu)
 };
 
 // Everything a kernel needs, passed by value.
@@ -74,6 +74,7 @@ struct Bufs {
     const float *seed_d;
     float *bound;  // forward: [p][n_rows] starting bounds of a seeded step (k_seed_bounds)
     int use_seeds;
+    int only_if_full;  // scoring kernels return at once unless st->full_scan is set (sorted first step)
 };
 
 constexpr int kPadCols = 64;     // row stride multiple of the feature-major arrays / D
@@ -105,6 +106,13 @@ cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s);
 constexpr int kSeedsPerLane = 8;        // seed columns each lane of the commit keeps
 constexpr int kSeeds = 32 * kSeedsPerLane;  // seed columns per row
 cudaError_t launch_commit(const Bufs &b, int backward, int *seeds, float *seed_d, cudaStream_t s);
+
+// First forward step of a holdout problem from per-feature sorted training
+// values (snn_sorted.cu): sort at load, then one thread per problem.
+size_t sort_temp_bytes(int p, int ldc);
+cudaError_t launch_sort_features(const Bufs &b, float *keys, int *vals, int *offsets, float *sv, int *si, void *temp,
+                                 size_t temp_bytes, cudaStream_t s);
+cudaError_t launch_first_step(const Bufs &b, const float *sv, const int *si, int n_cand, cudaStream_t s);
 
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);
 cudaError_t launch_init_forward(const Bufs &b, int cv, int npf, cudaStream_t s);

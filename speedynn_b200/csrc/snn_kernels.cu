@@ -296,7 +296,7 @@ __global__ void k_reset_state(Bufs b, int backward, int total_steps)
         s.n_cand = b.p;
         s.best_k_last = 0;
         s.num_final = backward ? b.p : 0;
-        s.pad = 0;
+        s.full_scan = 0;
         *b.st = s;
     }
 }

@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(512) k_score(Bufs b, int n_cand, int W, int n_
     const Layout S = carve(sm, WCC, K);
 
     if (b.st->done) return;
+    if (b.only_if_full && !b.st->full_scan) return;  // the sorted first step scored every problem
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int nthr = blockDim.x;

@@ -479,6 +479,7 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int
     constexpr bool LONG = KL > 32;
     const TmaSmem S = carve_tma<RG, CG>(smraw, KL, ring);
     if (b.st->done) return;
+    if (b.only_if_full && !b.st->full_scan) return;  // the sorted first step scored every problem
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int cgb = blockIdx.x % n_cg;

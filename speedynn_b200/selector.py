@@ -148,6 +148,10 @@ class Selector:
         """Scoring kernel: 0 automatic, 1 rows per lane (any k), 3 TMA-fed row tiles (k <= 64)."""
         check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_KERNEL, int(which)))
 
+    def set_sorted_start(self, enable):
+        """First forward holdout step from sorted feature columns (default on).  Results do not depend on it."""
+        check(_lib.lib().snn_set_option(self._h, _lib.SNN_OPT_SORTED_START, int(bool(enable))))
+
     def set_seed_step(self, step):
         """First forward step whose starting bounds come from seed columns (default 2, 3 for k > 16;
         a large value turns seeded steps off).  Results do not depend on it."""

@@ -393,3 +393,54 @@ def test_resume_from_committed_prefix_equals_uninterrupted_run(method):
         assert res["errors64"][i] == full["errors64"][i]
         assert res["step_best_k"][i] == full["step_best_k"][i]
     np.testing.assert_array_equal(res["mask"], full["mask"])
+
+
+def _first_step_data(kind, rng):
+    n_train, n_val, p = 3000, 700, 9
+    Xt = rng.normal(size=(n_train, p)).astype(np.float32)
+    Xv = rng.normal(size=(n_val, p)).astype(np.float32)
+    if kind == "duplicates":  # repeated training rows: tie groups of two and three
+        Xt[1000:1300] = Xt[:300]
+        Xt[2000:2100] = Xt[:100]
+    elif kind == "quantized":  # integer values: tie groups far larger than a thread orders
+        Xt = np.round(Xt * 2).astype(np.float32)
+        Xv = np.round(Xv * 2).astype(np.float32)
+    elif kind == "nonfinite":  # NaN and inf values never enter a list
+        Xt[::17, 2] = np.nan
+        Xt[::29, 4] = np.inf
+        Xv[::13, 4] = -np.inf
+        Xv[::31, 6] = np.nan
+    elif kind == "few_rows":  # k above the training rows: padded lists
+        Xt, n_train = Xt[:40], 40
+    yt = (Xt[:, 0] - 0.5 * np.nan_to_num(Xt[:, 1], posinf=0.0) + rng.normal(0, 0.1, n_train)).astype(np.float32)
+    yv = (Xv[:, 0] - 0.5 * Xv[:, 1] + rng.normal(0, 0.1, n_val)).astype(np.float32)
+    return Xt, yt, Xv, yv
+
+
+@pytest.mark.parametrize("kind", ["plain", "duplicates", "quantized", "nonfinite", "few_rows"])
+@pytest.mark.parametrize("kv", [[10], [3, 45]])
+def test_sorted_first_step_equals_scan(kind, kv):
+    """The first forward step from sorted feature columns against the scan of
+    every column: identical neighbour lists of every candidate and row, and
+    identical selections (quantized values exercise the hand-back to the scan)."""
+    rng = np.random.default_rng(101)
+    Xt, yt, Xv, yv = _first_step_data(kind, rng)
+    out = {}
+    for sorted_start in (True, False):
+        with Selector(Xt, yt, Xv, yv, k_vals=kv, num_features=3, method="forward") as sel:
+            sel.set_sorted_start(sorted_start)
+            r = sel.run()
+            sel.reset()
+            sel.keep_neighbours(True)
+            assert sel.step()
+            out[sorted_start] = (r, sel.neighbours())
+    (ra, na), (rb, nb) = out[True], out[False]
+    for k in ("ordering", "mask", "errors", "errors64", "step_best_k"):
+        np.testing.assert_array_equal(ra[k], rb[k])
+    for a, b in zip(na, nb):
+        np.testing.assert_array_equal(a, b)
+    if kind != "nonfinite":
+        prob = oracle.Problem(Xt, yt, Xv, yv)
+        o = oracle.select(prob, kv, 3, "forward")
+        np.testing.assert_array_equal(ra["ordering"], o["ordering"])
+        np.testing.assert_array_equal(ra["errors"], o["errors"])
