@@ -319,8 +319,10 @@ int issue_step(snn_handle *h, int t)
     if (use_tma(h)) {
         b.use_prev = backward && h->prev_ok ? 1 : 0;
         b.use_seeds = seeds_for_step(h, t) && h->seeds_ok ? 1 : 0;
-        b.inject_stall = h->inject_stall + 1;  // 0: off
-        h->inject_stall = -1;
+        if (!b.only_if_full) {  // the injected stall goes to a launch that scans
+            b.inject_stall = h->inject_stall + 1;  // 0: off
+            h->inject_stall = -1;
+        }
         if (b.use_seeds) {
             SNN_CUDA(snn::launch_seed_bounds(b, n_cand, h->stream));
             h->n_launch += 1;
