@@ -210,14 +210,16 @@ SNN_API int snn_get_timing(snn_handle *h, double *score_ms, int *score_launches,
  *                  only the work differs.  Default 2 (3 when k_max > 16); a
  *                  large value turns it off. */
 #define SNN_OPT_SEED_STEP 4
-/*   SNN_OPT_SORTED_START 1 (default): the first forward step of a holdout
- *                  problem (nothing committed yet, so every candidate's
- *                  distances are one-dimensional) takes each list from the
- *                  candidate's training values sorted at load: a binary search
- *                  and a short outward walk per (row, candidate) instead of a
- *                  scan; problems with more tied distances than it orders fall
- *                  back to the scan.  0: scan the first step too.  Results are
- *                  identical. */
+/*   SNN_OPT_SORTED_START 1 (default): the first two forward steps of a
+ *                  holdout problem take their lists from training values
+ *                  sorted at load instead of a scan.  Step 1 (nothing
+ *                  committed, every candidate's distances one-dimensional): a
+ *                  binary search and a short outward walk per (row,
+ *                  candidate).  Step 2 (one feature committed): a walk of that
+ *                  feature's sorted values in increasing committed distance,
+ *                  ended once it exceeds the candidate's k-th distance.  Data
+ *                  with too many tied distances fall back to the scan.  0:
+ *                  scan these steps too.  Results are identical. */
 #define SNN_OPT_SORTED_START 5
 SNN_API int snn_set_option(snn_handle *h, int option, int value);
 

@@ -103,6 +103,7 @@ struct snn_handle {
     int *sidx = nullptr, *sord = nullptr, *soff = nullptr;
     char *stemp = nullptr;
     size_t stemp_bytes = 0;
+    unsigned long long *walked = nullptr;  // columns walked by the sorted second step
     bool sorted_start = true;     // SNN_OPT_SORTED_START
     bool seeds_ok = false;        // seeds hold the current D's seed columns
     int seed_step = 2;            // SNN_OPT_SEED_STEP: first forward step scored from seed bounds (set at create)
@@ -226,7 +227,7 @@ void free_all(snn_handle *h)
         void *ptrs[] = {h->XT, h->cv ? nullptr : h->XV, h->yc, h->cv ? nullptr : h->yr, h->D, h->pred, h->rmse32,
                         h->err, h->stage, h->rmse64, h->err64, h->kv, h->cands, h->prev_cands, h->mask, h->order,
                         h->stepk, h->st, h->nn_idx, h->nn_dist, h->seeds, h->seed_d, h->sbound, h->sval, h->skey, h->sidx,
-                        h->sord, h->soff, h->stemp, h->perm, h->fvar,
+                        h->sord, h->soff, h->stemp, h->walked, h->perm, h->fvar,
                         h->d_loss_ids, h->lossval, h->err_all, h->kth_prev, h->dmax, h->fcount};
         for (void *q : ptrs)
             if (q) cudaFree(q);
@@ -288,9 +289,10 @@ bool seeds_for_step(const snn_handle *h, int t)
     return !h->desc.backward && h->seeds && use_tma(h) && t >= h->seed_step;
 }
 
-// The first forward step of a holdout problem runs from sorted feature columns
-// (D is still zero there); CV mode excludes same-fold pairs and takes the scan.
-bool sorted_step(const snn_handle *h, int t) { return t == 0 && h->sorted_start && h->sval && !h->desc.backward && !h->cv; }
+// The first two forward steps of a holdout problem run from sorted feature
+// columns (D is zero, then one-dimensional there); CV mode excludes same-fold
+// pairs and takes the scan.
+bool sorted_step(const snn_handle *h, int t) { return t <= 1 && h->sorted_start && h->sval && !h->desc.backward && !h->cv; }
 
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)
@@ -312,7 +314,8 @@ int issue_step(snn_handle *h, int t)
     }
     bool tma_step = false;
     if (sorted_step(h, t)) {
-        SNN_CUDA(snn::launch_first_step(b, h->sval, h->sidx, n_cand, h->stream));
+        if (t == 0) SNN_CUDA(snn::launch_first_step(b, h->sval, h->sidx, n_cand, h->stream));
+        else SNN_CUDA(snn::launch_second_step(b, h->sval, h->sidx, n_cand, h->walked, h->stream));
         b.only_if_full = 1;  // the scan below runs only if some tie group was too large
         h->n_launch += 1;
     }
@@ -556,6 +559,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
         if ((rc = dev_alloc(&h->soff, 2 * p, "sort offsets"))) return bail(rc);
         h->stemp_bytes = snn::sort_temp_bytes(h->p, h->ldc);
         if ((rc = dev_alloc(&h->stemp, h->stemp_bytes, "sort workspace"))) return bail(rc);
+        if ((rc = dev_alloc(&h->walked, 1, "walk counter"))) return bail(rc);
     }
     // On the handle's stream, so every kernel that reads k_vals comes after it
     // (the source lives as long as the handle).  A cudaMemcpy here would run on

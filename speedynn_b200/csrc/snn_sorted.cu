@@ -14,6 +14,8 @@
 // order (cpu.c:128-168).  The walk ends at k entries or at the first distance
 // >= FLT_MAX (such items never enter a list); the rest is padding (FLT_MAX, 0).
 // Then the kNN-mean predictions as the scoring kernels form them (cpu.c:56-66).
+// The second step walks the first winner's sorted values the same way
+// (k_second_step below).
 //
 // A tie group larger than kTieCap (e.g. integer-valued features with
 // thousands of equal values) is not resolved here: the thread raises
@@ -147,6 +149,123 @@ __global__ void __launch_bounds__(256) k_first_step(Bufs b, const float *sv, con
     }
 }
 
+// k_second_step: the second forward step of a holdout problem.  With one
+// feature w committed, D[r][i] = fl(fl(x_r,w - x_i,w)^2) is one-dimensional
+// again, so walking w's sorted values outwards from x_r,w (the smaller
+// frontier D first) visits the columns in increasing D.  Candidate c's
+// distance d = fl(D + fl((x_r,c - x_i,c)^2)) is at least D, so once the
+// frontier D exceeds the k-th distance of the list held so far no further
+// column can enter and the walk ends.  Columns arrive out of index order, so
+// the list is kept sorted by (distance, index), the reference's stable order.
+// D is recomputed from the sorted values (the same rounding the commit used),
+// not read from memory.
+//
+// Walks are usually short (on the fwd-64k data a median of ~1,000 columns of
+// 65,536) but not bounded: every warp adds its lanes' walked columns to a
+// global count every 256 steps, and once the count passes `budget` (an
+// eighth of a full scan) the kernel raises State::full_scan and every warp
+// leaves; the step's regular scoring launch then scans everything.
+template <int KL>
+__global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, const int *si, int n_cand,
+                                                     unsigned long long *walked, unsigned long long budget)
+{
+    if (b.st->done) return;
+    const unsigned kFull = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.y;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = slot < n_cand && r < b.n_rows;
+    const int K = b.kmax;
+    const int n = b.n_cols;
+    const int w = b.st->winner;
+    const int c = valid ? b.cands[slot] : 0;
+    const float aw = valid ? b.XV[(size_t)w * b.ldr + r] : 0.0f;
+    const float ac = valid ? b.XV[(size_t)c * b.ldr + r] : 0.0f;
+    const float *bv = sv + (size_t)w * b.ldc;
+    const int *bi = si + (size_t)w * b.ldc;
+    const float *xc = b.XT + (size_t)c * b.ldc;
+
+    float ld[KL];
+    int li[KL];
+    int cnt = 0;
+    // non-finite x_r,w or x_r,c: no distance below FLT_MAX, the list stays padding
+    bool active = valid && isfinite(aw) && isfinite(ac);
+    int L = -1, R = 0;
+    float dl = INFINITY, dr = INFINITY;
+    if (active) {
+        int lo = 0, hi = n;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (bv[mid] < aw) lo = mid + 1;
+            else hi = mid;
+        }
+        L = lo - 1;
+        R = lo;
+        dl = L >= 0 ? dist1(aw, bv[L]) : INFINITY;
+        dr = R < n ? dist1(aw, bv[R]) : INFINITY;
+    }
+    for (unsigned it = 1;; ++it) {
+        if ((it & 255u) == 0u) {  // account for the walk; leave when the budget is spent
+            const unsigned act = __popc(__ballot_sync(kFull, active));
+            int stop = 0;
+            if (lane == 0) {
+                const unsigned long long tot = atomicAdd(walked, 256ull * act) + 256ull * act;
+                if (tot > budget) atomicExch(&b.st->full_scan, 1);
+                stop = tot > budget || *(volatile int *)&b.st->full_scan;
+            }
+            if (__shfl_sync(kFull, stop, 0)) return;
+        }
+        if (!__any_sync(kFull, active)) break;
+        if (!active) continue;
+        const float dm = fminf(dl, dr);
+        if (!(dm < FLT_MAX) || (cnt == K && dm > ld[K - 1])) {
+            active = false;
+            continue;
+        }
+        int j;
+        if (dl <= dr) {
+            j = L--;
+            dl = L >= 0 ? dist1(aw, bv[L]) : INFINITY;
+        } else {
+            j = R++;
+            dr = R < n ? dist1(aw, bv[R]) : INFINITY;
+        }
+        const int i = bi[j];
+        const float t = __fsub_rn(ac, __ldg(xc + i));
+        const float d = __fadd_rn(dm, __fmul_rn(t, t));
+        if (d < FLT_MAX && (cnt < K || d < ld[K - 1] || (d == ld[K - 1] && i < li[K - 1]))) {
+            int q = cnt < K ? cnt++ : K - 1;  // the last entry drops out of a full list
+            while (q > 0 && (ld[q - 1] > d || (ld[q - 1] == d && li[q - 1] > i))) {
+                ld[q] = ld[q - 1];
+                li[q] = li[q - 1];
+                --q;
+            }
+            ld[q] = d;
+            li[q] = i;
+        }
+    }
+    if (!valid) return;
+    for (int j = cnt; j < K; ++j) {
+        ld[j] = FLT_MAX;
+        li[j] = 0;
+    }
+    if (b.nn_idx) {
+        const size_t o = ((size_t)slot * b.n_rows + r) * K;
+        for (int j = 0; j < K; ++j) {
+            b.nn_idx[o + j] = li[j];
+            b.nn_dist[o + j] = ld[j];
+        }
+    }
+    float acc = 0.0f;
+    for (int j = 0; j < K; ++j) {
+        acc = __fadd_rn(acc, __ldg(b.yc + li[j]));
+        for (int m = 0; m < b.nk; ++m) {
+            const int k = __ldg(b.kvals + m);
+            if (k == j + 1) b.pred[((size_t)slot * b.nk + m) * b.n_rows + r] = __fdiv_rn(acc, (float)k);
+        }
+    }
+}
+
 }  // namespace
 
 size_t sort_temp_bytes(int p, int ldc)
@@ -169,6 +288,19 @@ cudaError_t launch_sort_features(const Bufs &b, float *keys, int *vals, int *off
     if (e != cudaSuccess) return e;
     return cub::DeviceSegmentedRadixSort::SortPairs(temp, temp_bytes, keys, sv, vals, si, b.p * b.ldc, b.p, offsets,
                                                     offsets + b.p, 0, 32, s);
+}
+
+cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, int n_cand,
+                               unsigned long long *walked, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(walked, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    const unsigned long long budget = (unsigned long long)b.n_rows * (unsigned long long)n_cand * b.n_cols / 8;
+    const dim3 grid((b.n_rows + 255) / 256, n_cand);
+    if (b.kmax <= 16) k_second_step<16><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
+    else if (b.kmax <= 64) k_second_step<64><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
+    else k_second_step<kScoreMaxK><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_first_step(const Bufs &b, const float *sv, const int *si, int n_cand, cudaStream_t s)

@@ -419,10 +419,12 @@ def _first_step_data(kind, rng):
 
 @pytest.mark.parametrize("kind", ["plain", "duplicates", "quantized", "nonfinite", "few_rows"])
 @pytest.mark.parametrize("kv", [[10], [3, 45]])
-def test_sorted_first_step_equals_scan(kind, kv):
-    """The first forward step from sorted feature columns against the scan of
-    every column: identical neighbour lists of every candidate and row, and
-    identical selections (quantized values exercise the hand-back to the scan)."""
+def test_sorted_first_steps_equal_scan(kind, kv):
+    """The first two forward steps from sorted feature columns (a window
+    around each row's value, then a walk of the first winner's values) against
+    the scan of every column: identical neighbour lists of every candidate and
+    row at both steps, and identical selections (quantized values exercise the
+    hand-back to the scan)."""
     rng = np.random.default_rng(101)
     Xt, yt, Xv, yv = _first_step_data(kind, rng)
     out = {}
@@ -432,13 +434,17 @@ def test_sorted_first_step_equals_scan(kind, kv):
             r = sel.run()
             sel.reset()
             sel.keep_neighbours(True)
-            assert sel.step()
-            out[sorted_start] = (r, sel.neighbours())
-    (ra, na), (rb, nb) = out[True], out[False]
+            lists = []
+            for _ in range(2):
+                assert sel.step()
+                lists.append(sel.neighbours())
+            out[sorted_start] = (r, lists)
+    (ra, la), (rb, lb) = out[True], out[False]
     for k in ("ordering", "mask", "errors", "errors64", "step_best_k"):
         np.testing.assert_array_equal(ra[k], rb[k])
-    for a, b in zip(na, nb):
-        np.testing.assert_array_equal(a, b)
+    for na, nb in zip(la, lb):
+        for a, b in zip(na, nb):
+            np.testing.assert_array_equal(a, b)
     if kind != "nonfinite":
         prob = oracle.Problem(Xt, yt, Xv, yv)
         o = oracle.select(prob, kv, 3, "forward")
