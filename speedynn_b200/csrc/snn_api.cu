@@ -292,7 +292,11 @@ bool seeds_for_step(const snn_handle *h, int t)
 // The first two forward steps of a holdout problem run from sorted feature
 // columns (D is zero, then one-dimensional there); CV mode excludes same-fold
 // pairs and takes the scan.
-bool sorted_step(const snn_handle *h, int t) { return t == 0 && h->sorted_start && h->sval && !h->desc.backward && !h->cv; }
+bool sorted_step(const snn_handle *h, int t)
+{
+    if (!h->sorted_start || !h->sval || h->desc.backward || h->cv) return false;
+    return t == 0 || (t == 1 && h->kmax <= 64);  // the second step's walk keeps at most 64 entries
+}
 
 // Issue one greedy step (no synchronisation).
 int issue_step(snn_handle *h, int t)

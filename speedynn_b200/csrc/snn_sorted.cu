@@ -151,118 +151,168 @@ __global__ void __launch_bounds__(256) k_first_step(Bufs b, const float *sv, con
 
 // k_second_step: the second forward step of a holdout problem.  With one
 // feature w committed, D[r][i] = fl(fl(x_r,w - x_i,w)^2) is one-dimensional
-// again, so walking w's sorted values outwards from x_r,w (the smaller
-// frontier D first) visits the columns in increasing D.  Candidate c's
-// distance d = fl(D + fl((x_r,c - x_i,c)^2)) is at least D, so once the
-// frontier D exceeds the k-th distance of the list held so far no further
-// column can enter and the walk ends.  Columns arrive out of index order, so
-// the list is kept sorted by (distance, index), the reference's stable order.
-// D is recomputed from the sorted values (the same rounding the commit used),
-// not read from memory.
+// again: walking w's sorted values outwards from x_r,w visits each side's
+// columns in increasing D.  Candidate c's distance
+// d = fl(D + fl((x_r,c - x_i,c)^2)) is at least D, so a side is finished once
+// its next D exceeds the k-th distance of the list held so far.  One warp per
+// (candidate, row): each iteration lanes 0-15 take the next 16 columns on the
+// left, lanes 16-31 the next 16 on the right; columns whose D already exceeds
+// the k-th distance are not gathered, and the few that pass are inserted into
+// a register-held list (lane j holds entry j, and j + 32 when k > 32) sorted
+// by (distance, index) -- columns arrive out of index order, and that order
+// is the reference's stable one.  D is recomputed from the sorted values (the
+// commit's rounding), not read from memory.
 //
 // Walks are usually short (on the fwd-64k data a median of ~1,000 columns of
-// 65,536) but not bounded: every warp adds its lanes' walked columns to a
-// global count every 256 steps, and once the count passes `budget` (an
+// 65,536, ~32 iterations) but not bounded: a warp adds its columns to a
+// global count every 64 iterations, and once the count passes `budget` (an
 // eighth of a full scan) the kernel raises State::full_scan and every warp
 // leaves; the step's regular scoring launch then scans everything.
 template <int KL>
 __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, const int *si, int n_cand,
                                                      unsigned long long *walked, unsigned long long budget)
 {
+    constexpr bool LONG = KL > 32;
+    constexpr unsigned kFull = 0xffffffffu;
     if (b.st->done) return;
-    const unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int slot = blockIdx.y;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = slot < n_cand && r < b.n_rows;
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= n_cand || r >= b.n_rows) return;  // warp-uniform
     const int K = b.kmax;
     const int n = b.n_cols;
     const int w = b.st->winner;
-    const int c = valid ? b.cands[slot] : 0;
-    const float aw = valid ? b.XV[(size_t)w * b.ldr + r] : 0.0f;
-    const float ac = valid ? b.XV[(size_t)c * b.ldr + r] : 0.0f;
+    const int c = b.cands[slot];
+    const float aw = b.XV[(size_t)w * b.ldr + r];
+    const float ac = b.XV[(size_t)c * b.ldr + r];
     const float *bv = sv + (size_t)w * b.ldc;
     const int *bi = si + (size_t)w * b.ldc;
     const float *xc = b.XT + (size_t)c * b.ldc;
 
-    float ld[KL];
-    int li[KL];
+    // the list: entry e (e < cnt) at lane e (L0, I0) or lane e - 32 (L1, I1)
+    float L0 = INFINITY, L1 = INFINITY;
+    int I0 = 0x7fffffff, I1 = 0x7fffffff;
     int cnt = 0;
+    float th = INFINITY;  // the k-th entry once the list is full
+    int thi = 0x7fffffff;
     // non-finite x_r,w or x_r,c: no distance below FLT_MAX, the list stays padding
-    bool active = valid && isfinite(aw) && isfinite(ac);
-    int L = -1, R = 0;
-    float dl = INFINITY, dr = INFINITY;
-    if (active) {
+    if (isfinite(aw) && isfinite(ac)) {
         int lo = 0, hi = n;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             if (bv[mid] < aw) lo = mid + 1;
             else hi = mid;
         }
-        L = lo - 1;
-        R = lo;
-        dl = L >= 0 ? dist1(aw, bv[L]) : INFINITY;
-        dr = R < n ? dist1(aw, bv[R]) : INFINITY;
-    }
-    for (unsigned it = 1;; ++it) {
-        if ((it & 255u) == 0u) {  // account for the walk; leave when the budget is spent
-            const unsigned act = __popc(__ballot_sync(kFull, active));
-            int stop = 0;
-            if (lane == 0) {
-                const unsigned long long tot = atomicAdd(walked, 256ull * act) + 256ull * act;
-                if (tot > budget) atomicExch(&b.st->full_scan, 1);
-                stop = tot > budget || *(volatile int *)&b.st->full_scan;
+        int ln = lo - 1, rn = lo;  // next unvisited position on each side
+        bool ldone = ln < 0, rdone = rn >= n;
+        const bool left = lane < 16;
+        for (int it = 1; !(ldone && rdone); ++it) {
+            if ((it & 63) == 0) {  // account for the walk; leave when the budget is spent
+                int stop = 0;
+                if (lane == 0) {
+                    const unsigned long long tot = atomicAdd(walked, 64ull * 32ull) + 64ull * 32ull;
+                    if (tot > budget) atomicExch(&b.st->full_scan, 1);
+                    stop = tot > budget || *(volatile int *)&b.st->full_scan;
+                }
+                if (__shfl_sync(kFull, stop, 0)) return;
             }
-            if (__shfl_sync(kFull, stop, 0)) return;
-        }
-        if (!__any_sync(kFull, active)) break;
-        if (!active) continue;
-        const float dm = fminf(dl, dr);
-        if (!(dm < FLT_MAX) || (cnt == K && dm > ld[K - 1])) {
-            active = false;
-            continue;
-        }
-        int j;
-        if (dl <= dr) {
-            j = L--;
-            dl = L >= 0 ? dist1(aw, bv[L]) : INFINITY;
-        } else {
-            j = R++;
-            dr = R < n ? dist1(aw, bv[R]) : INFINITY;
-        }
-        const int i = bi[j];
-        const float t = __fsub_rn(ac, __ldg(xc + i));
-        const float d = __fadd_rn(dm, __fmul_rn(t, t));
-        if (d < FLT_MAX && (cnt < K || d < ld[K - 1] || (d == ld[K - 1] && i < li[K - 1]))) {
-            int q = cnt < K ? cnt++ : K - 1;  // the last entry drops out of a full list
-            while (q > 0 && (ld[q - 1] > d || (ld[q - 1] == d && li[q - 1] > i))) {
-                ld[q] = ld[q - 1];
-                li[q] = li[q - 1];
-                --q;
+            const int j = left ? ln - lane : rn + (lane - 16);
+            const bool in = left ? (!ldone && j >= 0) : (!rdone && j < n);
+            const float D = in ? dist1(aw, bv[j]) : INFINITY;
+            float d = INFINITY;
+            int i = 0x7fffffff;
+            if (in && D <= th) {  // d >= D: beyond the k-th distance nothing enters
+                i = bi[j];
+                const float t = __fsub_rn(ac, __ldg(xc + i));
+                d = __fadd_rn(D, __fmul_rn(t, t));
             }
-            ld[q] = d;
-            li[q] = i;
+            unsigned m = __ballot_sync(kFull, d < FLT_MAX && (d < th || (d == th && i < thi)));
+            while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                const float dv = __shfl_sync(kFull, d, l);
+                const int iv = __shfl_sync(kFull, i, l);
+                if (!(dv < th || (dv == th && iv < thi))) continue;  // the list tightened meanwhile
+                // position: entries ordered before (dv, iv)
+                int pos = __popc(__ballot_sync(kFull, lane < cnt && (L0 < dv || (L0 == dv && I0 < iv))));
+                const float up0 = __shfl_up_sync(kFull, L0, 1);
+                const int upi0 = __shfl_up_sync(kFull, I0, 1);
+                if constexpr (LONG) {
+                    pos += __popc(__ballot_sync(kFull, lane + 32 < cnt && (L1 < dv || (L1 == dv && I1 < iv))));
+                    float up1 = __shfl_up_sync(kFull, L1, 1);
+                    int upi1 = __shfl_up_sync(kFull, I1, 1);
+                    const float c31 = __shfl_sync(kFull, L0, 31);
+                    const int ci31 = __shfl_sync(kFull, I0, 31);
+                    if (lane == 0) {
+                        up1 = c31;
+                        upi1 = ci31;
+                    }
+                    if (lane + 32 == pos) {
+                        L1 = dv;
+                        I1 = iv;
+                    } else if (lane + 32 > pos && lane + 32 < K) {
+                        L1 = up1;
+                        I1 = upi1;
+                    }
+                }
+                if (lane == pos) {
+                    L0 = dv;
+                    I0 = iv;
+                } else if (lane > pos && lane < K) {
+                    L0 = up0;
+                    I0 = upi0;
+                }
+                if (cnt < K) ++cnt;
+                if (cnt == K) {
+                    if constexpr (LONG) {
+                        th = K <= 32 ? __shfl_sync(kFull, L0, (K - 1) & 31) : __shfl_sync(kFull, L1, (K - 33) & 31);
+                        thi = K <= 32 ? __shfl_sync(kFull, I0, (K - 1) & 31) : __shfl_sync(kFull, I1, (K - 33) & 31);
+                    } else {
+                        th = __shfl_sync(kFull, L0, K - 1);
+                        thi = __shfl_sync(kFull, I0, K - 1);
+                    }
+                }
+            }
+            // a side is finished past its end or once its farthest D of this batch exceeds the k-th
+            const float dl_far = __shfl_sync(kFull, D, 15), dr_far = __shfl_sync(kFull, D, 31);
+            ln -= 16;
+            rn += 16;
+            ldone = ldone || ln < 0 || dl_far > th;
+            rdone = rdone || rn >= n || dr_far > th;
         }
     }
-    if (!valid) return;
-    for (int j = cnt; j < K; ++j) {
-        ld[j] = FLT_MAX;
-        li[j] = 0;
+    // entries past cnt are padding (FLT_MAX, 0)
+    if (lane >= cnt) {
+        L0 = FLT_MAX;
+        I0 = 0;
+    }
+    if (lane + 32 >= cnt) {
+        L1 = FLT_MAX;
+        I1 = 0;
     }
     if (b.nn_idx) {
         const size_t o = ((size_t)slot * b.n_rows + r) * K;
-        for (int j = 0; j < K; ++j) {
-            b.nn_idx[o + j] = li[j];
-            b.nn_dist[o + j] = ld[j];
+        if (lane < K) {
+            b.nn_idx[o + lane] = I0;
+            b.nn_dist[o + lane] = L0;
+        }
+        if (LONG && lane + 32 < K) {
+            b.nn_idx[o + lane + 32] = I1;
+            b.nn_dist[o + lane + 32] = L1;
         }
     }
+    // labels summed in rank order (sequential FP32) by lane 0, as the scoring kernels
+    const float y0 = lane < K ? __ldg(b.yc + I0) : 0.0f;
+    const float y1 = LONG && lane + 32 < K ? __ldg(b.yc + I1) : 0.0f;
     float acc = 0.0f;
-    for (int j = 0; j < K; ++j) {
-        acc = __fadd_rn(acc, __ldg(b.yc + li[j]));
-        for (int m = 0; m < b.nk; ++m) {
-            const int k = __ldg(b.kvals + m);
-            if (k == j + 1) b.pred[((size_t)slot * b.nk + m) * b.n_rows + r] = __fdiv_rn(acc, (float)k);
-        }
+    for (int e = 0; e < K; ++e) {
+        const float ye = e < 32 ? __shfl_sync(kFull, y0, e) : __shfl_sync(kFull, y1, e - 32);
+        acc = __fadd_rn(acc, ye);
+        if (lane == 0)
+            for (int m = 0; m < b.nk; ++m) {
+                const int k = __ldg(b.kvals + m);
+                if (k == e + 1) b.pred[((size_t)slot * b.nk + m) * b.n_rows + r] = __fdiv_rn(acc, (float)k);
+            }
     }
 }
 
@@ -296,10 +346,10 @@ cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, in
     cudaError_t e = cudaMemsetAsync(walked, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
     const unsigned long long budget = (unsigned long long)b.n_rows * (unsigned long long)n_cand * b.n_cols / 8;
-    const dim3 grid((b.n_rows + 255) / 256, n_cand);
-    if (b.kmax <= 16) k_second_step<16><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
+    const dim3 grid((b.n_rows + 7) / 8, n_cand);  // a warp per (candidate, row)
+    if (b.kmax <= 32) k_second_step<32><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
     else if (b.kmax <= 64) k_second_step<64><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
-    else k_second_step<kScoreMaxK><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
+    else return cudaErrorInvalidValue;  // k above 64 scans
     return cudaGetLastError();
 }
 
