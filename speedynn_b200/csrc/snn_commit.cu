@@ -111,10 +111,15 @@ __global__ void __launch_bounds__(256, 4) k_commit(Bufs b, int *seeds, float *se
                     }
                     __stcs(row + q, d[u]);
                     if (SEEDS) {
-                        keep_n(sv, si, d[u].x, 4 * q);
-                        keep_n(sv, si, d[u].y, 4 * q + 1);
-                        keep_n(sv, si, d[u].z, 4 * q + 2);
-                        keep_n(sv, si, d[u].w, 4 * q + 3);
+                        // entries are rare once the list holds near columns: one
+                        // test per float4 keeps the insertion code off the common path
+                        const float lim = sv[kSeedsPerLane - 1];
+                        if (fminf(fminf(d[u].x, d[u].y), fminf(d[u].z, d[u].w)) < lim) {
+                            keep_n(sv, si, d[u].x, 4 * q);
+                            keep_n(sv, si, d[u].y, 4 * q + 1);
+                            keep_n(sv, si, d[u].z, 4 * q + 2);
+                            keep_n(sv, si, d[u].w, 4 * q + 3);
+                        }
                     }
                 }
             }
