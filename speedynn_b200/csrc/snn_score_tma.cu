@@ -159,16 +159,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned by
                  "r"(bytes)
                  : "memory");
 }
-// try_wait with a suspend-time hint: a warp whose stage is not ready sleeps in
-// hardware until the phase completes (or the hint runs out) instead of
-// spinning on issue slots the scheduler's working warps need.
-constexpr unsigned kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
 {
     unsigned ok;
-    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
                  : "=r"(ok)
-                 : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendNs)
+                 : "r"(smem_addr(bar)), "r"(parity)
                  : "memory");
     return ok != 0;
 }
@@ -179,9 +175,7 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 // Bounded wait: gives up after kSpinLimit polls or one second of wall time,
-// whichever comes first (a stage normally completes within microseconds; a
-// poll suspends for at most kSuspendNs, so the time check every 256 polls
-// comes at least every ~5 ms).
+// whichever comes first (a stage normally completes within microseconds).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
 {
     if (mbar_try_wait(bar, parity)) return true;
