@@ -156,7 +156,8 @@ __global__ void __launch_bounds__(256) k_first_step(Bufs b, const float *sv, con
 // d = fl(D + fl((x_r,c - x_i,c)^2)) is at least D, so a side is finished once
 // its next D exceeds the k-th distance of the list held so far.  One warp per
 // (candidate, row): each iteration lanes 0-15 take the next 16 columns on the
-// left, lanes 16-31 the next 16 on the right; columns whose D already exceeds
+// left, lanes 16-31 the next 16 on the right (all 32 lanes the open side once
+// the other is finished); columns whose D already exceeds
 // the k-th distance are not gathered, and the few that pass are inserted into
 // a register-held list (lane j holds entry j, and j + 32 when k > 32) sorted
 // by (distance, index) -- columns arrive out of index order, and that order
@@ -205,7 +206,6 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
         }
         int ln = lo - 1, rn = lo;  // next unvisited position on each side
         bool ldone = ln < 0, rdone = rn >= n;
-        const bool left = lane < 16;
         for (int it = 1; !(ldone && rdone); ++it) {
             if ((it & 63) == 0) {  // account for the walk; leave when the budget is spent
                 int stop = 0;
@@ -216,8 +216,11 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
                 }
                 if (__shfl_sync(kFull, stop, 0)) return;
             }
-            const int j = left ? ln - lane : rn + (lane - 16);
-            const bool in = left ? (!ldone && j >= 0) : (!rdone && j < n);
+            // 16 columns per side, or all 32 lanes on the side still open
+            const int nl = ldone ? 0 : (rdone ? 32 : 16);
+            const bool left = lane < nl;
+            const int j = left ? ln - lane : rn + (lane - nl);
+            const bool in = left ? j >= 0 : (!rdone && j < n);
             const float D = in ? dist1(aw, bv[j]) : INFINITY;
             float d = INFINITY;
             int i = 0x7fffffff;
@@ -274,11 +277,11 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
                 }
             }
             // a side is finished past its end or once its farthest D of this batch exceeds the k-th
-            const float dl_far = __shfl_sync(kFull, D, 15), dr_far = __shfl_sync(kFull, D, 31);
-            ln -= 16;
-            rn += 16;
-            ldone = ldone || ln < 0 || dl_far > th;
-            rdone = rdone || rn >= n || dr_far > th;
+            const float dl_far = __shfl_sync(kFull, D, nl > 0 ? nl - 1 : 0), dr_far = __shfl_sync(kFull, D, 31);
+            ln -= nl;
+            rn += 32 - nl;
+            ldone = ldone || ln < 0 || (nl > 0 && dl_far > th);
+            rdone = rdone || rn >= n || (nl < 32 && dr_far > th);
         }
     }
     // entries past cnt are padding (FLT_MAX, 0)
