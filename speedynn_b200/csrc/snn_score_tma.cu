@@ -379,7 +379,7 @@ __device__ __forceinline__ float warp_kth(float (&v)[V], int K, int lane)
 // have their K-th smallest distance at or above the final K-th neighbour
 // distance, so it is an inclusive bound; padding seeds (index -1) and NaN
 // distances count as +inf.  One warp per row, lane l holding seeds
-// l + 32 j (j < kSeedsPerLane); the gathers of four candidates are issued
+// l + 32 j (j < kSeedsPerLane); the gathers of two candidates are issued
 // together, and many warps per SM hide their latency.  Each lane keeps its
 // V smallest values (V = 2 for K <= 16, 4 above), and the K-th smallest of
 // those 32 V values is the bound: a subset of the seeds, so still K distinct
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(256) k_seed_bounds(Bufs b, int n_cand, float *
         si[j] = __ldg(b.seeds + (size_t)r * kSeeds + j * 32 + lane);
         sd[j] = __ldg(b.seed_d + (size_t)r * kSeeds + j * 32 + lane);
     }
-    constexpr int Q = 4;  // candidates whose gathers are in flight together
+    constexpr int Q = 2;  // candidates whose gathers are in flight together (4: 96 registers, no faster)
     for (int c0 = 0; c0 < n_cand; c0 += Q) {
         int cid[Q];
         float xr[Q], g[Q][S];
