@@ -7,7 +7,9 @@ mode and would take hours to days single-threaded), so the oracle
 host cores, and this script stores the result:
 
     fwd-64k   forward, 65,536 train x 32,768 validation rows, p=60, k=10, all 15 steps
-    bwd-50k   backward, 50,000 x 25,000 rows, p=120 -> 20, k=5, all 100 removals
+    bwd-50k   backward, 50,000 x 25,000 rows, p=120 -> 20, k=5, the first STEPS_BWD
+              removals (the restatement rebuilds each row's 120-feature distance every
+              removal, so all 100 would take it most of a day)
     fwd-200k  forward, 200,000 x 100,000 rows, p=100, k=50, 2 % duplicated rows,
               the first STEPS_200K steps (the whole run would take the oracle days)
 
@@ -21,7 +23,9 @@ generator change from a selection mismatch.
 
     python tests/golden/make_config_golden.py [fwd-64k] [bwd-50k] [fwd-200k] [--threads N]
 
-Minutes to hours of CPU time per workload (fwd-64k about 20 minutes on 8 cores).
+Minutes to hours of CPU time per workload (fwd-64k about 20 minutes on 8 cores).  A fixture
+that covers only the first steps of a run stores ``steps`` below the run's; its tests compare
+those steps.
 """
 import argparse
 import hashlib
@@ -39,6 +43,7 @@ from oracle import oracle  # noqa: E402
 from speedynn_b200 import datagen  # noqa: E402
 
 STEPS_200K = 2
+STEPS_BWD = 10
 
 
 def data_sha256(split):
@@ -58,8 +63,12 @@ def make(name, threads):
     split, k, select = datagen.workload(name)
     backward = name.startswith("bwd")
     p = split.Xtrain.shape[1]
-    steps = p - select if backward else (STEPS_200K if name == "fwd-200k" else select)
-    nf = select if backward else steps
+    if backward:
+        steps = min(STEPS_BWD, p - select)
+        nf = p - steps
+    else:
+        steps = STEPS_200K if name == "fwd-200k" else select
+        nf = steps
     prob = oracle.Problem(split.Xtrain, split.ytrain, split.Xval, split.yval)
     t0 = time.time()
     o = oracle.select(prob, [k], nf, "backward" if backward else "forward", nthreads=threads)
@@ -75,7 +84,9 @@ def make(name, threads):
         full64[t] = np.sqrt(sq.sum() / sq.size)
     t_64 = time.time() - t0
     out = os.path.join(HERE, f"config_{name.replace('-', '')}.npz")
+    full_steps = p - select if backward else select
     np.savez_compressed(out, workload=name, data_sha256=data_sha256(split), k=k, steps=steps,
+                        run_steps=full_steps,
                         method="backward" if backward else "forward", num_features=nf,
                         ordering=o["ordering"], mask=o["mask"], errors=o["errors"], errors64=o["errors64"],
                         step_best_k=o["step_best_k"], best_k=o["best_k"], num_final=o["num_final"],
