@@ -42,7 +42,7 @@ sys.path.insert(0, ROOT)
 from oracle import oracle  # noqa: E402
 from speedynn_b200 import datagen  # noqa: E402
 
-STEPS_200K = 2
+STEPS_200K = 4
 STEPS_BWD = 10
 
 

@@ -4,7 +4,7 @@ Each workload is generated at full size and run on the GPU with the library's
 default options.  Two checks per workload:
 
 * the whole selection (for bwd-50k its first 10 removals, for fwd-200k its
-  first 2 steps) against the oracle's run of the same inputs, stored by
+  first 4 steps) against the oracle's run of the same inputs, stored by
   tests/golden/make_config_golden.py
   (ordering, mask, best k per step and FP32 errors bit for bit; FP64 errors
   within 1e-9 relative);
