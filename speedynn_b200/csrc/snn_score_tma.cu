@@ -26,9 +26,11 @@
 //     computed beforehand by k_seed_bounds; or, on
 //     backward steps after the first, the previous step's k-th distances
 //     (kth_prev), which removal only lowers.
-//   * Full pass: a conservative sign-bit filter (one sub and one FMA per
-//     evaluation; filter_bound / filter_bound_bwd) flags rows that may hold a
-//     passing column; flagged rows are re-scored with the reference's
+//   * Full pass: forward, 64-column chunks whose committed distances all
+//     exceed the warp's row bounds are skipped (d >= D); in the rest a
+//     conservative sign-bit filter (one sub and one FMA per evaluation;
+//     filter_bound / filter_bound_bwd) flags rows that may hold a passing
+//     column; flagged rows are re-scored with the reference's
 //     rounding and passes are inserted in column order (d <= T until the list
 //     is full, then d < k-th).
 //   * Every wait is bounded: on timeout the warp records SNN_ERR_TIMEOUT in
@@ -724,20 +726,30 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int
                 for (int q = 0; q < kSC / kChunk; ++q) {
                     if (q >= nch) break;
                     const int q0 = q * kChunk;
-                    float2 dp[kRW], xp[kCW];
+                    float2 dp[kRW], E[kRW], xp[kCW];
 #pragma unroll
-                    for (int ri = 0; ri < kRW; ++ri) dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0);
+                    for (int ri = 0; ri < kRW; ++ri) {
+                        dp[ri] = *reinterpret_cast<const float2 *>(D_w + ri * kSC + q0);
+                        E[ri] = BWD ? sub2(H2[ri], dp[ri]) : sub2(dp[ri], H2[ri]);
+                    }
+                    if constexpr (!BWD) {
+                        // Forward, d = fl(D + fl(t*t)) >= D: a column passes only if
+                        // D <= T < H, i.e. fl(D - H) < 0 for one of the warp's rows.
+                        unsigned a = 0u;
+#pragma unroll
+                        for (int ri = 0; ri < kRW; ++ri) a |= f2u(E[ri].x) | f2u(E[ri].y);
+                        if (!__any_sync(kFull, (int)a < 0)) continue;
+                    }
 #pragma unroll
                     for (int ci = 0; ci < kCW; ++ci) xp[ci] = *reinterpret_cast<const float2 *>(X_w + ci * kSC + q0);
                     unsigned acc[kRW];
 #pragma unroll
                     for (int ri = 0; ri < kRW; ++ri) {
-                        const float2 E = BWD ? sub2(H2[ri], dp[ri]) : sub2(dp[ri], H2[ri]);
                         float2 u[kCW];
 #pragma unroll
                         for (int ci = 0; ci < kCW; ++ci) {
                             const float2 t = sub2(xv2[ri * kCW + ci], xp[ci]);
-                            u[ci] = fma2(t, t, E);
+                            u[ci] = fma2(t, t, E[ri]);
                         }
                         if constexpr (BWD)
                             acc[ri] = (f2u(u[0].x) & f2u(u[0].y) & f2u(u[1].x)) & (f2u(u[1].y) & f2u(u[2].x) & f2u(u[2].y)) &
