@@ -4,17 +4,18 @@
 // d_i = fl(D[r,i] +/- fl((x_r,c - x_i,c)^2)) over the training columns i in
 // the reference's stable (distance, index) order
 // (speedynn/lib/cpu.c:128-168) and the kNN-mean predictions (cpu.c:56-66).
-// A block scores 24 rows x 12 candidates; each of its 18 consumer warps owns 4
-// rows x 4 candidates and walks the columns two per lane with packed f32x2
-// (18 consumers + 1 producer = 19 warps, at most 5 per SM sub-partition at 96
-// registers; 12-candidate groups leave no padded slot for 60 candidates).
-// For 32 < k <= 64 the 64-slot lists (two entries per lane) take more shared
+// A block scores 24 (forward with k <= 16: 12) rows x 12 candidates; each of
+// its 18 (9) consumer warps owns 4 rows x 4 candidates and walks the columns
+// two per lane with packed f32x2 (19 warps per block, or two blocks of 10
+// warps per SM: at most 5 warps per SM sub-partition at 96 registers;
+// 12-candidate groups leave no padded slot for 60 candidates).  For
+// 32 < k <= 64 the 64-slot lists (two entries per lane) take more shared
 // memory, which leaves room for a 2-slot ring.
 //
 //   * Feed: one producer lane streams 256-column stages into a ring of
 //     shared-memory slots (as deep as fits beside the lists): a 2-D
-//     tensor-map TMA copy of the 24 D rows and three tile::gather4 copies
-//     of the 12 candidate rows of X, all completing on the stage's "full"
+//     tensor-map TMA copy of the block's D rows and three tile::gather4
+//     copies of the 12 candidate rows of X, all completing on the stage's "full"
 //     mbarrier; consumers release a slot through its "empty" mbarrier, so a
 //     warp busy inserting falls behind by up to a ring of stages without
 //     stalling the others.
@@ -58,7 +59,7 @@ static_assert(2 * kMaxRing * sizeof(uint64_t) <= kBarBytes, "mbarriers must fit 
 // A block has RG x CG consumer warps (template arguments), each owning kRW
 // rows x kCW candidates: kRowsB = RG * kRW scored rows, kCandB = CG * kCW
 // candidates, kConsumers = RG * CG.
-constexpr int kRingDeep = 5;      // ring slots beside 16-slot lists (k <= 16)
+constexpr int kRingDeep = 5;      // ring slots beside 16-slot lists (k <= 16, backward)
 constexpr int kRingShallow = 4;   // ring slots beside 32- and 64-slot lists
 constexpr int kRW = 4, kCW = 4, kP = kRW * kCW;
 constexpr long long kSpinLimit = 1ll << 22;  // try_wait polls before giving up
@@ -472,7 +473,7 @@ __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL, int ri
 // and two first-pass minima per lane.
 // (32, 64] -- two list entries per lane and two first-pass minima per lane.
 template <bool BWD, int ring, bool COUNT, int RG, int CG, int KL>
-__global__ void __launch_bounds__((RG * CG + 1) * 32, 1) k_score_tma(Bufs b, int n_cand, int n_cg,
+__global__ void __launch_bounds__((RG * CG + 1) * 32, RG * CG <= 9 ? 2 : 1) k_score_tma(Bufs b, int n_cand, int n_cg,
                                                                      const __grid_constant__ CUtensorMap tmD,
                                                                      const __grid_constant__ CUtensorMap tmX)
 {
@@ -927,12 +928,17 @@ cudaError_t launch_shape(const Bufs &b, int n_cand, int max_smem, cudaStream_t s
 template <bool BWD, bool COUNT>
 cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 {
-    // 24-row x 12-candidate blocks throughout: 16-slot lists leave room for a
-    // 5-slot ring, 32-slot lists for 4 slots, 64-slot lists (k <= 64) for 2
-    // (measured on k = 50: 19 warps with 2 slots beat 16 warps with 3 and 13
-    // warps with 4).
+    // 12-candidate blocks throughout.  Forward with 16-slot lists: 12-row
+    // blocks with a 3-slot ring, two blocks per SM (a block waits for its
+    // slowest warp, and the other block's warps fill the gap; fwd-64k 376.8 ->
+    // 367.1 ms per selection against one 24-row block); backward keeps one
+    // 24-row block with a 5-slot ring (bwd-50k 1710 against 1754 ms).  32-slot
+    // lists leave room for 4 slots, 64-slot lists (k <= 64) for 2 (measured on
+    // k = 50: 19 warps with 2 slots beat 16 warps with 3 and 13 warps with 4).
     switch (list_slots(b.kmax)) {
-    case 16: return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, max_smem, s);
+    case 16:
+        if constexpr (BWD) return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, max_smem, s);
+        else return launch_shape<BWD, COUNT, 3, 3, 3, 16>(b, n_cand, max_smem, s);
     case 32: return launch_shape<BWD, COUNT, kRingShallow, 6, 3, 32>(b, n_cand, max_smem, s);
     default: return launch_shape<BWD, COUNT, 2, 6, 3, 64>(b, n_cand, max_smem, s);
     }
