@@ -319,7 +319,7 @@ int issue_step(snn_handle *h, int t)
     bool tma_step = false;
     if (sorted_step(h, t)) {
         if (t == 0) SNN_CUDA(snn::launch_first_step(b, h->sval, h->sidx, n_cand, h->stream));
-        else SNN_CUDA(snn::launch_second_step(b, h->sval, h->sidx, n_cand, h->walked, h->stream));
+        else SNN_CUDA(snn::launch_second_step(b, h->sval, h->sidx, h->skey, n_cand, h->walked, h->stream));
         b.only_if_full = 1;  // the scan below runs only if some tie group was too large
         h->n_launch += 1;
     }
@@ -557,6 +557,7 @@ SNN_API int snn_create(const snn_desc *d, snn_handle **out)
     if (!d->backward && !cv) {
         const size_t pl = p * h->ldc;
         if ((rc = dev_alloc(&h->sval, pl, "sorted values"))) return bail(rc);
+        // the sort's keys at load, then the second step's candidate values in sorted order
         if ((rc = dev_alloc(&h->skey, pl, "sort keys"))) return bail(rc);
         if ((rc = dev_alloc(&h->sidx, pl, "sorted indices"))) return bail(rc);
         if ((rc = dev_alloc(&h->sord, pl, "sort values"))) return bail(rc);

@@ -113,8 +113,10 @@ size_t sort_temp_bytes(int p, int ldc);
 cudaError_t launch_sort_features(const Bufs &b, float *keys, int *vals, int *offsets, float *sv, int *si, void *temp,
                                  size_t temp_bytes, cudaStream_t s);
 cudaError_t launch_first_step(const Bufs &b, const float *sv, const int *si, int n_cand, cudaStream_t s);
-// The second step: walks of the first winner's sorted values (walked: a device counter).
-cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, int n_cand,
+// The second step: walks of the first winner's sorted values (xs: n_cand x ldc
+// floats of scratch for the candidates' values in that order; walked: a device
+// counter).
+cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, float *xs, int n_cand,
                                unsigned long long *walked, cudaStream_t s);
 
 cudaError_t launch_transpose(const float *X, int n, int p, float *XT, int ld, cudaStream_t s);

@@ -158,20 +158,37 @@ __global__ void __launch_bounds__(256) k_first_step(Bufs b, const float *sv, con
 // (candidate, row): each iteration lanes 0-15 take the next 16 columns on the
 // left, lanes 16-31 the next 16 on the right (all 32 lanes the open side once
 // the other is finished); columns whose D already exceeds
-// the k-th distance are not gathered, and the few that pass are inserted into
+// the k-th distance are skipped, and the few that pass are inserted into
 // a register-held list (lane j holds entry j, and j + 32 when k > 32) sorted
 // by (distance, index) -- columns arrive out of index order, and that order
 // is the reference's stable one.  D is recomputed from the sorted values (the
-// commit's rounding), not read from memory.
+// commit's rounding), not read from memory, and the candidates' values come
+// from xs, X's candidate rows put in w's sorted column order beforehand
+// (k_gather_sorted), so every load of the walk is contiguous and none waits
+// for another.
 //
 // Walks are usually short (on the fwd-64k data a median of ~1,000 columns of
 // 65,536, ~32 iterations) but not bounded: a warp adds its columns to a
 // global count every 64 iterations, and once the count passes `budget` (an
 // eighth of a full scan) the kernel raises State::full_scan and every warp
 // leaves; the step's regular scoring launch then scans everything.
+// xs[slot][j] = X[c][i_j] for the step's candidates c = cands[slot] and w's
+// sorted columns i_j (w = the first step's winner).
+__global__ void __launch_bounds__(256) k_gather_sorted(Bufs b, const int *si, float *xs, int n_cand)
+{
+    if (b.st->done) return;
+    const int slot = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= n_cand || j >= b.n_cols) return;
+    const int w = b.st->winner;
+    const int c = b.cands[slot];
+    xs[(size_t)slot * b.ldc + j] = __ldg(b.XT + (size_t)c * b.ldc + __ldg(si + (size_t)w * b.ldc + j));
+}
+
 template <int KL>
-__global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, const int *si, int n_cand,
-                                                     unsigned long long *walked, unsigned long long budget)
+__global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, const int *si, const float *xs,
+                                                     int n_cand, unsigned long long *walked,
+                                                     unsigned long long budget)
 {
     constexpr bool LONG = KL > 32;
     constexpr unsigned kFull = 0xffffffffu;
@@ -188,7 +205,7 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
     const float ac = b.XV[(size_t)c * b.ldr + r];
     const float *bv = sv + (size_t)w * b.ldc;
     const int *bi = si + (size_t)w * b.ldc;
-    const float *xc = b.XT + (size_t)c * b.ldc;
+    const float *xsc = xs + (size_t)slot * b.ldc;
 
     // the list: entry e (e < cnt) at lane e (L0, I0) or lane e - 32 (L1, I1)
     float L0 = INFINITY, L1 = INFINITY;
@@ -221,12 +238,15 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
             const bool left = lane < nl;
             const int j = left ? ln - lane : rn + (lane - nl);
             const bool in = left ? j >= 0 : (!rdone && j < n);
-            const float D = in ? dist1(aw, bv[j]) : INFINITY;
+            // the three loads are independent (and contiguous across the lanes)
+            const float vj = in ? bv[j] : 0.0f, xj = in ? xsc[j] : 0.0f;
+            const int ij = in ? bi[j] : 0x7fffffff;
+            const float D = in ? dist1(aw, vj) : INFINITY;
             float d = INFINITY;
             int i = 0x7fffffff;
             if (in && D <= th) {  // d >= D: beyond the k-th distance nothing enters
-                i = bi[j];
-                const float t = __fsub_rn(ac, __ldg(xc + i));
+                i = ij;
+                const float t = __fsub_rn(ac, xj);
                 d = __fadd_rn(D, __fmul_rn(t, t));
             }
             unsigned m = __ballot_sync(kFull, d < FLT_MAX && (d < th || (d == th && i < thi)));
@@ -343,15 +363,16 @@ cudaError_t launch_sort_features(const Bufs &b, float *keys, int *vals, int *off
                                                     offsets + b.p, 0, 32, s);
 }
 
-cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, int n_cand,
+cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, float *xs, int n_cand,
                                unsigned long long *walked, cudaStream_t s)
 {
     cudaError_t e = cudaMemsetAsync(walked, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
+    k_gather_sorted<<<dim3((b.n_cols + 255) / 256, n_cand), 256, 0, s>>>(b, si, xs, n_cand);
     const unsigned long long budget = (unsigned long long)b.n_rows * (unsigned long long)n_cand * b.n_cols / 8;
     const dim3 grid((b.n_rows + 7) / 8, n_cand);  // a warp per (candidate, row)
-    if (b.kmax <= 32) k_second_step<32><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
-    else if (b.kmax <= 64) k_second_step<64><<<grid, 256, 0, s>>>(b, sv, si, n_cand, walked, budget);
+    if (b.kmax <= 32) k_second_step<32><<<grid, 256, 0, s>>>(b, sv, si, xs, n_cand, walked, budget);
+    else if (b.kmax <= 64) k_second_step<64><<<grid, 256, 0, s>>>(b, sv, si, xs, n_cand, walked, budget);
     else return cudaErrorInvalidValue;  // k above 64 scans
     return cudaGetLastError();
 }
