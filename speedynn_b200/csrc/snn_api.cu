@@ -321,7 +321,7 @@ int issue_step(snn_handle *h, int t)
         if (t == 0) SNN_CUDA(snn::launch_first_step(b, h->sval, h->sidx, n_cand, h->stream));
         else SNN_CUDA(snn::launch_second_step(b, h->sval, h->sidx, h->skey, n_cand, h->walked, h->stream));
         b.only_if_full = 1;  // the scan below runs only if some tie group was too large
-        h->n_launch += 1;
+        h->n_launch += t == 0 ? 1 : 2;  // the second step gathers the candidates in sorted order first
     }
     if (use_tma(h)) {
         b.use_prev = backward && h->prev_ok ? 1 : 0;
@@ -331,8 +331,9 @@ int issue_step(snn_handle *h, int t)
             h->inject_stall = -1;
         }
         if (b.use_seeds) {
-            SNN_CUDA(snn::launch_seed_bounds(b, n_cand, h->stream));
-            h->n_launch += 1;
+            // the sort's value buffer (p x ldc, unused after load) holds the row-major candidates
+            SNN_CUDA(snn::launch_seed_bounds(b, n_cand, reinterpret_cast<float *>(h->sord), h->stream));
+            h->n_launch += h->kmax <= 16 && h->sord ? 2 : 1;
         }
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
         h->prev_ok = backward && h->kth_prev;  // this step wrote every candidate's k-th distances

@@ -99,7 +99,9 @@ void clear_error();
 bool score_tma_supported(int kmax);  // kernel option 3: k_max <= 64
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
 // Seeded forward steps: each candidate's starting bound from the seed columns, into b.bound.
-cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s);
+// xrm: n_cols x n_cand floats of scratch (the candidates' columns row-major),
+// or null to take the bounds from part of the seeds (k_seed_bounds).
+cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, float *xrm, cudaStream_t s);
 
 // Commit the winner into D (snn_commit.cu); forward commits given seed
 // buffers also keep kSeeds near columns per row for the next step's bounds.

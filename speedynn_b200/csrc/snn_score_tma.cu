@@ -375,6 +375,77 @@ __device__ __forceinline__ float warp_kth(float (&v)[V], int K, int lane)
     return __shfl_sync(kFull, sel, (K - 1) / V);
 }
 
+// xrm[i][slot] = X[cands[slot]][i]: the step's candidate columns, row-major
+// (n_cols x n_cand), through 32 x 32 shared-memory tiles.
+__global__ void __launch_bounds__(256) k_candidates_rowmajor(Bufs b, int n_cand, float *xrm)
+{
+    __shared__ float tile[32][33];
+    if (b.st->done) return;
+    const int i0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = ty; k < 32; k += 8) {
+        const int slot = s0 + k, i = i0 + tx;
+        tile[k][tx] = slot < n_cand && i < b.n_cols ? __ldg(b.XT + (size_t)__ldg(b.cands + slot) * b.ldc + i) : 0.0f;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int i = i0 + k, slot = s0 + tx;
+        if (i < b.n_cols && slot < n_cand) xrm[(size_t)i * n_cand + slot] = tile[tx][k];
+    }
+}
+
+// k_seed_bounds_exact (K <= 16): the bound of each (candidate, scored row)
+// problem is the K-th smallest exact distance d = fl(D + fl((x_r,c - x_i,c)^2))
+// over ALL kSeeds seed columns of the row (see k_seed_bounds for why any K
+// distinct columns bound the final K-th distance).  One warp per row, lane l
+// taking candidate slot l (then l + 32, ...): the 16 smallest distances seen
+// sit sorted in registers, and each seed column's values for 32 candidates
+// are one contiguous read of xrm.  Seeds are taken in the commit's order;
+// a seed whose committed distance already reaches every lane's 16th smallest
+// is skipped (d >= D).
+__global__ void __launch_bounds__(256) k_seed_bounds_exact(Bufs b, int n_cand, const float *xrm, float *bound)
+{
+    constexpr int L = 16;
+    if (b.st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (r >= b.n_rows) return;  // warp-uniform
+    const int K = b.kmax;
+    for (int c0 = 0; c0 < n_cand; c0 += 32) {
+        const int slot = c0 + lane;
+        const bool live = slot < n_cand;
+        const int c = live ? __ldg(b.cands + slot) : 0;  // the candidate feature
+        const float xv = live ? __ldg(b.XV + (size_t)c * b.ldr + r) : 0.0f;
+        float l[L];
+#pragma unroll
+        for (int j = 0; j < L; ++j) l[j] = INFINITY;
+        for (int j0 = 0; j0 < kSeeds; j0 += 32) {
+            const int myi = __ldg(b.seeds + (size_t)r * kSeeds + j0 + lane);
+            const float myd = __ldg(b.seed_d + (size_t)r * kSeeds + j0 + lane);
+            for (int jj = 0; jj < 32; ++jj) {
+                const int i = __shfl_sync(kFull, myi, jj);
+                const float D = __shfl_sync(kFull, myd, jj);
+                if (i < 0 || !__any_sync(kFull, D < l[L - 1])) continue;  // padding seed, or no lane can take it
+                const float x = live ? __ldg(xrm + (size_t)i * n_cand + slot) : 0.0f;
+                const float t = __fsub_rn(xv, x);
+                float d = __fadd_rn(D, __fmul_rn(t, t));
+                if (!(d < FLT_MAX) || !live) d = INFINITY;  // NaN or overflow: never a neighbour
+                if (__any_sync(kFull, d < l[L - 1])) {
+                    // keep the L smallest sorted: l[j] = min(l[j], max(l[j-1], d))
+#pragma unroll
+                    for (int j = L - 1; j > 0; --j) l[j] = fminf(l[j], fmaxf(l[j - 1], d));
+                    l[0] = fminf(l[0], d);
+                }
+            }
+        }
+        float kth = l[0];
+#pragma unroll
+        for (int j = 1; j < L; ++j)
+            if (j == K - 1) kth = l[j];
+        if (live) bound[(size_t)c * b.n_rows + r] = kth;  // indexed by feature, as k_seed_bounds
+    }
+}
+
 // k_seed_bounds: the starting bound of every (candidate, scored row) problem
 // of a seeded forward step, bound[c][r] = the K-th smallest exact distance
 // d = fl(D + fl((x_r,c - x_i,c)^2)) over columns of the row's kSeeds seed
@@ -623,7 +694,7 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, RG * CG <= 9 ? 2 : 1) k_sc
         for (int p = 0; p < kP; ++p) mn[p] = mn2[p] = INFINITY;
         for (int v = 0; v < nA && alive; ++v) {
             const int s = v % ring;
-            if (!mbar_wait(S.full + s, (v / ring) & 1)) {
+            if (!__all_sync(kFull, mbar_wait(S.full + s, (v / ring) & 1))) {  // warp-uniform: collectives follow
                 alive = false;
                 break;
             }
@@ -712,7 +783,7 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, RG * CG <= 9 ? 2 : 1) k_sc
         for (int ri = 0; ri < kRW; ++ri) H2[ri] = row_H(ri);
         for (int v = nA; v < nvirt && alive; ++v) {
             const int s = v % ring;
-            if (!mbar_wait(S.full + s, (v / ring) & 1)) {
+            if (!__all_sync(kFull, mbar_wait(S.full + s, (v / ring) & 1))) {  // warp-uniform: collectives follow
                 alive = false;
                 break;
             }
@@ -946,9 +1017,14 @@ cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 
 }  // namespace
 
-cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, cudaStream_t s)
+cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, float *xrm, cudaStream_t s)
 {
     const int grid = (b.n_rows + 7) / 8;
+    if (b.kmax <= 16 && xrm) {
+        k_candidates_rowmajor<<<dim3((b.n_cols + 31) / 32, (n_cand + 31) / 32), 256, 0, s>>>(b, n_cand, xrm);
+        k_seed_bounds_exact<<<grid, 256, 0, s>>>(b, n_cand, xrm, b.bound);
+        return cudaGetLastError();
+    }
     if (b.kmax > 16) k_seed_bounds<4><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
     else k_seed_bounds<2><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
     return cudaGetLastError();
