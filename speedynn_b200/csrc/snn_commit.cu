@@ -59,10 +59,12 @@ __device__ __forceinline__ void keep_n(float (&s)[N], int (&i)[N], float v, int 
     }
 }
 
-// At most 64 registers (4 blocks of 256 threads per SM): the stream needs
-// the warps to keep enough loads in flight to stay HBM-bound.
+// Three blocks of 256 threads per SM, each lane with four float4 loads of D in
+// flight: the stream needs that many bytes in flight to stay HBM-bound (four
+// blocks with two loads per lane while the seed lists take registers: 44.0
+// against 43.0 ms of commits per fwd-64k selection).
 template <bool BWD, bool SEEDS>
-__global__ void __launch_bounds__(256, 4) k_commit(Bufs b, int *seeds, float *seed_d)
+__global__ void __launch_bounds__(256, 3) k_commit(Bufs b, int *seeds, float *seed_d)
 {
     if (b.st->done) return;
     const int lane = threadIdx.x & 31;
@@ -82,8 +84,7 @@ __global__ void __launch_bounds__(256, 4) k_commit(Bufs b, int *seeds, float *se
             sv[j] = INFINITY;
             si[j] = -1;
         }
-        // U float4 per lane in flight (2 when the seed lists take registers)
-        constexpr int U = SEEDS ? 2 : 4;
+        constexpr int U = 4;  // float4 loads per lane in flight
         for (int q0 = 0; q0 < n4; q0 += 32 * U) {
             float4 d[U], c[U];
 #pragma unroll
@@ -151,7 +152,7 @@ int sm_count_commit()
 cudaError_t launch_commit(const Bufs &b, int backward, int *seeds, float *seed_d, cudaStream_t s)
 {
     int grid = (b.n_rows + 7) / 8;
-    const int cap = sm_count_commit() * 8;
+    const int cap = sm_count_commit() * 6;
     if (grid > cap) grid = cap;
     if (backward) k_commit<true, false><<<grid, 256, 0, s>>>(b, nullptr, nullptr);
     else if (seeds && seed_d) k_commit<false, true><<<grid, 256, 0, s>>>(b, seeds, seed_d);
