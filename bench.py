@@ -49,9 +49,9 @@ import numpy as np  # noqa: E402
 WORKLOAD = "fwd-64k"
 # DRAM bytes per (validation row, training row) pair of one scoring launch, from an
 # ncu capture of a seeded step (dram__bytes_read.sum + dram__bytes_write.sum =
-# 544.6 + 5.8 MB for 8192 x 16384 pairs): the D stream read once plus the small
+# 544.2 + 8.3 MB for 8192 x 16384 pairs): the D stream read once plus the small
 # X, bound and label traffic.
-TRAFFIC_PER_PAIR = 550.48e6 / (8192 * 16384)
+TRAFFIC_PER_PAIR = 552.44e6 / (8192 * 16384)
 METRIC = "cand-evals/s (n_val*n_train*candidates per second), greedy forward selection"
 UNIT = "cand-evals/s"
 
@@ -532,7 +532,7 @@ def run_ours(args, world, rank, local):
                          "traffic": args.traffic if args.traffic is not None else TRAFFIC_PER_PAIR * n_val * n_train,
                          "traffic_source": "command line" if args.traffic is not None else
                          "ncu dram__bytes_read.sum + dram__bytes_write.sum of one seeded k_score_tma launch on "
-                         "the 16384 x 8192 case (550.5 MB, profiles/k_score_tma_small_ncu.md), scaled per "
+                         "the 16384 x 8192 case (552.4 MB, profiles/k_score_tma_small_ncu.md), scaled per "
                          "(validation row, training row) pair"},
             "clocks": clocks,
             "result": {"ordering": [int(x) for x in res["ordering"][:steps]],
