@@ -394,18 +394,18 @@ __global__ void __launch_bounds__(256) k_candidates_rowmajor(Bufs b, int n_cand,
     }
 }
 
-// k_seed_bounds_exact (K <= 16): the bound of each (candidate, scored row)
+// k_seed_bounds_exact (K <= L <= 16): the bound of each (candidate, scored row)
 // problem is the K-th smallest exact distance d = fl(D + fl((x_r,c - x_i,c)^2))
 // over ALL kSeeds seed columns of the row (see k_seed_bounds for why any K
 // distinct columns bound the final K-th distance).  One warp per row, lane l
-// taking candidate slot l (then l + 32, ...): the 16 smallest distances seen
-// sit sorted in registers, and each seed column's values for 32 candidates
+// taking candidate slot l (then l + 32, ...): the L smallest distances seen
+// sit sorted in registers (L the list length rounded up to 4, 8, 12 or 16), and each seed column's values for 32 candidates
 // are one contiguous read of xrm.  Seeds are taken in the commit's order;
-// a seed whose committed distance already reaches every lane's 16th smallest
+// a seed whose committed distance already reaches every lane's L-th smallest
 // is skipped (d >= D).
+template <int L>
 __global__ void __launch_bounds__(256) k_seed_bounds_exact(Bufs b, int n_cand, const float *xrm, float *bound)
 {
-    constexpr int L = 16;
     if (b.st->done) return;
     const int lane = threadIdx.x & 31;
     const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -1022,7 +1022,10 @@ cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, float *xrm, cudaStream
     const int grid = (b.n_rows + 7) / 8;
     if (b.kmax <= 16 && xrm) {
         k_candidates_rowmajor<<<dim3((b.n_cols + 31) / 32, (n_cand + 31) / 32), 256, 0, s>>>(b, n_cand, xrm);
-        k_seed_bounds_exact<<<grid, 256, 0, s>>>(b, n_cand, xrm, b.bound);
+        if (b.kmax <= 4) k_seed_bounds_exact<4><<<grid, 256, 0, s>>>(b, n_cand, xrm, b.bound);
+        else if (b.kmax <= 8) k_seed_bounds_exact<8><<<grid, 256, 0, s>>>(b, n_cand, xrm, b.bound);
+        else if (b.kmax <= 12) k_seed_bounds_exact<12><<<grid, 256, 0, s>>>(b, n_cand, xrm, b.bound);
+        else k_seed_bounds_exact<16><<<grid, 256, 0, s>>>(b, n_cand, xrm, b.bound);
         return cudaGetLastError();
     }
     if (b.kmax > 16) k_seed_bounds<4><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
