@@ -575,6 +575,7 @@ def run_plain(probs, batch_res, evals, batch_ms, world):
     plain_ms = 0.0
     same = True
     best_rate = 0.0
+    by_k = {}  # k -> [evaluations, ms]: the plain form's rate per list length
     for pr, rb in zip(probs, batch_res):
         with Selector(pr["Xtrain"], pr["ytrain"], pr["Xval"], pr["yval"], k_vals=pr["k_vals"],
                       num_features=pr["num_features"], method=pr["method"]) as sel:
@@ -583,12 +584,16 @@ def run_plain(probs, batch_res, evals, batch_ms, world):
             plain_ms += ms
         e = cand_evals(pr["Xval"].shape[0], pr["Xtrain"].shape[0], pr["Xtrain"].shape[1], pr["num_features"])
         best_rate = max(best_rate, e / (ms / 1000.0))
+        acc = by_k.setdefault(int(max(pr["k_vals"])), [0.0, 0.0])
+        acc[0] += e
+        acc[1] += ms
         same = same and np.array_equal(r["ordering"], rb["ordering"]) and np.array_equal(r["errors"], rb["errors"])
     # a batch can at best run every problem at the rate the best single problem reaches alone
     ceiling_ms = 1000.0 * evals / best_rate
     return {"ms": plain_ms, "value": world * evals / (plain_ms / 1000.0), "batched_speedup": plain_ms / batch_ms,
             "identical_results": bool(same), "best_single_problem_rate": best_rate,
             "ceiling_ms": ceiling_ms, "ceiling_speedup": plain_ms / ceiling_ms,
+            "rate_by_k": {str(k): v[0] / (v[1] / 1000.0) for k, v in sorted(by_k.items())},
             "note": "the problems one at a time (CUDA-event time of each selection, creates and uploads excluded); "
                     "ceiling: all evaluations at the best single problem's own rate"}
 
@@ -619,6 +624,7 @@ def batch_summary(args, local):
             "plain_ms": plain["ms"], "plain_value": plain["value"], "batched_speedup": plain["batched_speedup"],
             "identical_results": plain["identical_results"], "ceiling_speedup": plain["ceiling_speedup"],
             "best_single_problem_rate": plain["best_single_problem_rate"],
+            "plain_rate_by_k": plain["rate_by_k"],
             "note": "batch_ms: union of the problems' CUDA-event intervals; batch_e2e: snn_batch_run wall time "
                     "(creates, uploads, runs, result reads, frees); plain: each problem's own selection time"}
 
