@@ -336,6 +336,7 @@ int issue_step(snn_handle *h, int t)
             h->n_launch += h->kmax <= 16 && h->sord ? 2 : 1;
         }
         SNN_CUDA(snn::launch_score_tma(b, n_cand, backward, h->stream));
+        h->n_launch += snn::score_tma_launches(h->kmax, n_cand, backward) - 1;  // counted once below
         h->prev_ok = backward && h->kth_prev;  // this step wrote every candidate's k-th distances
         tma_step = true;
     } else {

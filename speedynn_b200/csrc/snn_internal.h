@@ -98,6 +98,7 @@ void clear_error();
 // Warp-specialised TMA scoring (snn_score_tma.cu), k_max <= 64.
 bool score_tma_supported(int kmax);  // kernel option 3: k_max <= 64
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s);
+int score_tma_launches(int kmax, int n_cand, int backward);  // kernels one launch_score_tma issues
 // Seeded forward steps: each candidate's starting bound from the seed columns, into b.bound.
 // xrm: n_cols x n_cand floats of scratch (the candidates' columns row-major),
 // or null to take the bounds from part of the seeds (k_seed_bounds).

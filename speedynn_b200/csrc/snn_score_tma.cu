@@ -544,7 +544,7 @@ __device__ __forceinline__ TmaSmem carve_tma(unsigned char *base, int KL, int ri
 // and two first-pass minima per lane.
 // (32, 64] -- two list entries per lane and two first-pass minima per lane.
 template <bool BWD, int ring, bool COUNT, int RG, int CG, int KL>
-__global__ void __launch_bounds__((RG * CG + 1) * 32, RG * CG <= 9 ? 2 : 1) k_score_tma(Bufs b, int n_cand, int n_cg,
+__global__ void __launch_bounds__((RG * CG + 1) * 32, RG * CG <= 9 ? 2 : 1) k_score_tma(Bufs b, int n_cand, int n_cg, int slot0,
                                                                      const __grid_constant__ CUtensorMap tmD,
                                                                      const __grid_constant__ CUtensorMap tmX)
 {
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__((RG * CG + 1) * 32, RG * CG <= 9 ? 2 : 1) k_sc
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int cgb = blockIdx.x % n_cg;
     const int r0 = (blockIdx.x / n_cg) * kRowsB;
-    const int c0 = cgb * kCandB;
+    const int c0 = slot0 + cgb * kCandB;  // the block's first candidate slot
 
     if (threadIdx.x < kCandB) {
         const int s = c0 + threadIdx.x;
@@ -976,11 +976,12 @@ bool encode_rows(CUtensorMap *m, const float *base, int ld, long long rows, int 
 
 namespace {
 
+// One launch over candidate slots [slot0, slot0 + n_slots) of the step's n_cand.
 template <bool BWD, bool COUNT, int RING, int RG, int CG, int KL>
-cudaError_t launch_shape(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
+cudaError_t launch_shape(const Bufs &b, int n_cand, int slot0, int n_slots, int max_smem, cudaStream_t s)
 {
     constexpr int kRowsB = RG * kRW, kCandB = CG * kCW;
-    const int n_cg = (n_cand + kCandB - 1) / kCandB;
+    const int n_cg = (n_slots + kCandB - 1) / kCandB;
     const long long blocks = (long long)((b.n_rows + kRowsB - 1) / kRowsB) * n_cg;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     CUtensorMap tmD, tmX;
@@ -992,26 +993,49 @@ cudaError_t launch_shape(const Bufs &b, int n_cand, int max_smem, cudaStream_t s
     auto kern = k_score_tma<BWD, RING, COUNT, RG, CG, KL>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(unsigned)blocks, (RG * CG + 1) * 32, smem, s>>>(b, n_cand, n_cg, tmD, tmX);
+    kern<<<(unsigned)blocks, (RG * CG + 1) * 32, smem, s>>>(b, n_cand, n_cg, slot0, tmD, tmX);
     return cudaGetLastError();
+}
+
+// Forward with 16-slot lists: the remainder of n_cand over 12-candidate groups
+// gets its own launch with fewer candidates and more rows per block, so that
+// no block holds idle candidate warps (a block takes as long as its busiest
+// warp, so a block with one of three candidate warps busy costs about as much
+// as a full one).  1 or 2: the number of launches.
+int remainder_shape(int kmax, int n_cand, int backward)
+{
+    if (backward || list_slots(kmax) != 16) return 0;
+    const int rem = n_cand % 12;
+    if (n_cand < 12 || rem == 0 || rem > 8) return 0;
+    return rem <= 4 ? 1 : 2;  // candidate warps per block of the remainder launch
 }
 
 template <bool BWD, bool COUNT>
 cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
 {
-    // 12-candidate blocks throughout.  Forward with 16-slot lists: 12-row
-    // blocks with a 3-slot ring, two blocks per SM (a block waits for its
-    // slowest warp, and the other block's warps fill the gap; fwd-64k 376.8 ->
-    // 367.1 ms per selection against one 24-row block); backward keeps one
+    // 12-candidate blocks.  Forward with 16-slot lists: 12-row blocks with a
+    // 3-slot ring, two blocks per SM (a block waits for its slowest warp, and
+    // the other block's warps fill the gap; fwd-64k 376.8 -> 367.1 ms per
+    // selection against one 24-row block); the remainder candidates in
+    // 36-row x 4-candidate or 16-row x 8-candidate blocks.  Backward keeps one
     // 24-row block with a 5-slot ring (bwd-50k 1710 against 1754 ms).  32-slot
     // lists leave room for 4 slots, 64-slot lists (k <= 64) for 2 (measured on
     // k = 50: 19 warps with 2 slots beat 16 warps with 3 and 13 warps with 4).
     switch (list_slots(b.kmax)) {
     case 16:
-        if constexpr (BWD) return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, max_smem, s);
-        else return launch_shape<BWD, COUNT, 3, 3, 3, 16>(b, n_cand, max_smem, s);
-    case 32: return launch_shape<BWD, COUNT, kRingShallow, 6, 3, 32>(b, n_cand, max_smem, s);
-    default: return launch_shape<BWD, COUNT, 2, 6, 3, 64>(b, n_cand, max_smem, s);
+        if constexpr (BWD) {
+            return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, 0, n_cand, max_smem, s);
+        } else {
+            const int rs = remainder_shape(b.kmax, n_cand, 0);
+            if (rs == 0) return launch_shape<BWD, COUNT, 3, 3, 3, 16>(b, n_cand, 0, n_cand, max_smem, s);
+            const int n_full = n_cand - n_cand % 12;
+            cudaError_t e = launch_shape<BWD, COUNT, 3, 3, 3, 16>(b, n_cand, 0, n_full, max_smem, s);
+            if (e != cudaSuccess) return e;
+            if (rs == 1) return launch_shape<BWD, COUNT, 2, 9, 1, 16>(b, n_cand, n_full, n_cand - n_full, max_smem, s);
+            return launch_shape<BWD, COUNT, 3, 4, 2, 16>(b, n_cand, n_full, n_cand - n_full, max_smem, s);
+        }
+    case 32: return launch_shape<BWD, COUNT, kRingShallow, 6, 3, 32>(b, n_cand, 0, n_cand, max_smem, s);
+    default: return launch_shape<BWD, COUNT, 2, 6, 3, 64>(b, n_cand, 0, n_cand, max_smem, s);
     }
 }
 
@@ -1032,6 +1056,8 @@ cudaError_t launch_seed_bounds(const Bufs &b, int n_cand, float *xrm, cudaStream
     else k_seed_bounds<2><<<grid, 256, 0, s>>>(b, n_cand, b.bound);
     return cudaGetLastError();
 }
+
+int score_tma_launches(int kmax, int n_cand, int backward) { return remainder_shape(kmax, n_cand, backward) ? 2 : 1; }
 
 cudaError_t launch_score_tma(const Bufs &b, int n_cand, int backward, cudaStream_t s)
 {
