@@ -997,14 +997,15 @@ cudaError_t launch_shape(const Bufs &b, int n_cand, int slot0, int n_slots, int 
     return cudaGetLastError();
 }
 
-// Forward with 16-slot lists: the remainder of n_cand over 12-candidate groups
-// gets its own launch with fewer candidates and more rows per block, so that
-// no block holds idle candidate warps (a block takes as long as its busiest
-// warp, so a block with one of three candidate warps busy costs about as much
-// as a full one).  1 or 2: the number of launches.
-int remainder_shape(int kmax, int n_cand, int backward)
+// With 16-slot lists the remainder of n_cand over 12-candidate groups (1 to 8
+// candidates) gets its own launch with fewer candidates and more rows per
+// block, so that no block holds idle candidate warps (a block takes as long as
+// its busiest warp, so a block with one of three candidate warps busy costs
+// about as much as a full one).  Returns 0 (one launch) or the remainder
+// blocks' candidate warps, 1 or 2.
+int remainder_shape(int kmax, int n_cand, int)
 {
-    if (backward || list_slots(kmax) != 16) return 0;
+    if (list_slots(kmax) != 16) return 0;
     const int rem = n_cand % 12;
     if (n_cand < 12 || rem == 0 || rem > 8) return 0;
     return rem <= 4 ? 1 : 2;  // candidate warps per block of the remainder launch
@@ -1018,13 +1019,20 @@ cudaError_t launch_k(const Bufs &b, int n_cand, int max_smem, cudaStream_t s)
     // the other block's warps fill the gap; fwd-64k 376.8 -> 367.1 ms per
     // selection against one 24-row block); the remainder candidates in
     // 36-row x 4-candidate or 16-row x 8-candidate blocks.  Backward keeps one
-    // 24-row block with a 5-slot ring (bwd-50k 1710 against 1754 ms).  32-slot
+    // 24-row block per SM with a 5-slot ring (bwd-50k 1710 against 1754 ms);
+    // its remainder in 72-row x 4-candidate or 36-row x 8-candidate blocks.  32-slot
     // lists leave room for 4 slots, 64-slot lists (k <= 64) for 2 (measured on
     // k = 50: 19 warps with 2 slots beat 16 warps with 3 and 13 warps with 4).
     switch (list_slots(b.kmax)) {
     case 16:
         if constexpr (BWD) {
-            return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, 0, n_cand, max_smem, s);
+            const int rs = remainder_shape(b.kmax, n_cand, 1);
+            if (rs == 0) return launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, 0, n_cand, max_smem, s);
+            const int n_full = n_cand - n_cand % 12;
+            cudaError_t e = launch_shape<BWD, COUNT, kRingDeep, 6, 3, 16>(b, n_cand, 0, n_full, max_smem, s);
+            if (e != cudaSuccess) return e;
+            if (rs == 1) return launch_shape<BWD, COUNT, 2, 18, 1, 16>(b, n_cand, n_full, n_cand - n_full, max_smem, s);
+            return launch_shape<BWD, COUNT, 4, 9, 2, 16>(b, n_cand, n_full, n_cand - n_full, max_smem, s);
         } else {
             const int rs = remainder_shape(b.kmax, n_cand, 0);
             if (rs == 0) return launch_shape<BWD, COUNT, 3, 3, 3, 16>(b, n_cand, 0, n_cand, max_smem, s);
