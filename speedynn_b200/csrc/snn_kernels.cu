@@ -155,20 +155,33 @@ __global__ void __launch_bounds__(kReduceWarps * 32) k_reduce(Bufs b, int n_cand
     const float *pr = b.pred + (size_t)w * b.n_rows;
     float s32 = 0.0f;
     double s64 = 0.0;
+    constexpr int Q = kReduceChunk / 32;
+    // the next chunk's values are loaded while lane 0 sums the current one
+    float pv[Q], yv[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int rr = q * 32 + lane;
+        pv[q] = rr < b.n_rows ? pr[rr] : 0.0f;
+        yv[q] = rr < b.n_rows ? b.yr[rr] : 0.0f;
+    }
     for (int base = 0; base < b.n_rows; base += kReduceChunk) {
 #pragma unroll
-        for (int q = 0; q < kReduceChunk / 32; ++q) {
+        for (int q = 0; q < Q; ++q) {
             const int rr = base + q * 32 + lane;
             if (rr < b.n_rows) {
-                const float pv = pr[rr];
-                const float yv = b.yr[rr];
-                const float e = __fsub_rn(yv, pv);
+                const float e = __fsub_rn(yv[q], pv[q]);
                 sq[wl][q * 32 + lane] = __fmul_rn(e, e);
-                const double e64 = (double)yv - (double)pv;
+                const double e64 = (double)yv[q] - (double)pv[q];
                 s64 += e64 * e64;
             }
         }
         __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int rr = base + kReduceChunk + q * 32 + lane;
+            pv[q] = rr < b.n_rows ? pr[rr] : 0.0f;
+            yv[q] = rr < b.n_rows ? b.yr[rr] : 0.0f;
+        }
         if (lane == 0) {
             const int cnt = min(kReduceChunk, b.n_rows - base);
             for (int t = 0; t < cnt; ++t) s32 = __fadd_rn(s32, sq[wl][t]);
