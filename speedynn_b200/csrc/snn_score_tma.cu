@@ -422,19 +422,28 @@ __global__ void __launch_bounds__(256) k_seed_bounds_exact(Bufs b, int n_cand, c
         for (int j0 = 0; j0 < kSeeds; j0 += 32) {
             const int myi = __ldg(b.seeds + (size_t)r * kSeeds + j0 + lane);
             const float myd = __ldg(b.seed_d + (size_t)r * kSeeds + j0 + lane);
-            for (int jj = 0; jj < 32; ++jj) {
-                const int i = __shfl_sync(kFull, myi, jj);
-                const float D = __shfl_sync(kFull, myd, jj);
-                if (i < 0 || !__any_sync(kFull, D < l[L - 1])) continue;  // padding seed, or no lane can take it
-                const float x = live ? __ldg(xrm + (size_t)i * n_cand + slot) : 0.0f;
-                const float t = __fsub_rn(xv, x);
-                float d = __fadd_rn(D, __fmul_rn(t, t));
-                if (!(d < FLT_MAX) || !live) d = INFINITY;  // NaN or overflow: never a neighbour
-                if (__any_sync(kFull, d < l[L - 1])) {
-                    // keep the L smallest sorted: l[j] = min(l[j], max(l[j-1], d))
+            // eight seeds at a time: their loads are issued together, then inserted in order
+            for (int j8 = 0; j8 < 32; j8 += 8) {
+                int ii[8];
+                float DD[8], xx[8];
 #pragma unroll
-                    for (int j = L - 1; j > 0; --j) l[j] = fminf(l[j], fmaxf(l[j - 1], d));
-                    l[0] = fminf(l[0], d);
+                for (int u = 0; u < 8; ++u) {
+                    ii[u] = __shfl_sync(kFull, myi, j8 + u);
+                    DD[u] = __shfl_sync(kFull, myd, j8 + u);
+                    xx[u] = live && ii[u] >= 0 ? __ldg(xrm + (size_t)ii[u] * n_cand + slot) : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const float t = __fsub_rn(xv, xx[u]);
+                    float d = __fadd_rn(DD[u], __fmul_rn(t, t));
+                    // padding seed, NaN or overflow: never a neighbour
+                    if (!(d < FLT_MAX) || !live || ii[u] < 0) d = INFINITY;
+                    if (__any_sync(kFull, d < l[L - 1])) {
+                        // keep the L smallest sorted: l[j] = min(l[j], max(l[j-1], d))
+#pragma unroll
+                        for (int j = L - 1; j > 0; --j) l[j] = fminf(l[j], fmaxf(l[j - 1], d));
+                        l[0] = fminf(l[0], d);
+                    }
                 }
             }
         }
