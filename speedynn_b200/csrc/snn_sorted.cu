@@ -59,6 +59,21 @@ __device__ __forceinline__ float dist1(float a, float b)
 }
 
 // Sorted insertion of column index v into ix[0..n) (ascending).
+// Ascending bitonic sort of one 64-bit key per lane over the warp.
+__device__ __forceinline__ unsigned long long warp_sort64(unsigned long long key, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            key = keep_min ? (o < key ? o : key) : (o > key ? o : key);
+        }
+    }
+    return key;
+}
+
 __device__ __forceinline__ void insert_idx(int *ix, int n, int v)
 {
     int j = n;
@@ -249,7 +264,25 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
                 const float t = __fsub_rn(ac, xj);
                 d = __fadd_rn(D, __fmul_rn(t, t));
             }
-            unsigned m = __ballot_sync(kFull, d < FLT_MAX && (d < th || (d == th && i < thi)));
+            const bool fill = cnt == 0;
+            if (fill) {
+                // the first batch fills the empty list at once: its finite distances
+                // sorted by (distance, index) (distances are >= +0, so their bits
+                // order like the values), the first K kept
+                const unsigned long long key =
+                    d < FLT_MAX ? ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)i : ~0ull;
+                const unsigned long long srt = warp_sort64(key, lane);
+                cnt = min(__popc(__ballot_sync(kFull, d < FLT_MAX)), K);
+                if (lane < cnt) {
+                    L0 = __uint_as_float((unsigned)(srt >> 32));
+                    I0 = (int)(unsigned)(srt & 0xffffffffu);
+                }
+                if (cnt == K) {  // K <= 32 here
+                    th = __shfl_sync(kFull, L0, (K - 1) & 31);
+                    thi = __shfl_sync(kFull, I0, (K - 1) & 31);
+                }
+            }
+            unsigned m = fill ? 0u : __ballot_sync(kFull, d < FLT_MAX && (d < th || (d == th && i < thi)));
             while (m) {
                 const int l = __ffs(m) - 1;
                 m &= m - 1;
