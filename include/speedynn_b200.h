@@ -313,10 +313,14 @@ SNN_API int snn_batch_destroy(snn_batch *b);
  * are: the scorer's exact filter relies on it.  stream: a cudaStream_t
  * (NULL = legacy default stream); the call waits for it.
  *
- * The first call on each device looks up the scratch's device address
- * (with that device current); make that first call before any stream
- * capture.  All calls share the scratch and it keeps the last call's
- * contents: calls whose GPU work overlaps race on it. */
+ * The scratch is placed on a GPU when the CUDA runtime loads this library's
+ * kernels there (lazily: at the first call of any library entry point on
+ * that GPU), so a caller with a strict no-allocation window makes one call
+ * per GPU before the window opens.  Every call looks up the scratch's device
+ * address with the device current (it can move after a device reset); make
+ * the first call on a device before any stream capture.  All calls share the
+ * scratch and it keeps the last call's contents: calls whose GPU work
+ * overlaps race on it. */
 SNN_API int snn_score_step_noalloc(const float *D, int ld, const float *XT, const float *XV, int ldr,
                                    const float *y_train, const float *y_val, int n_rows, int n_train, int p,
                                    const int *cands, int n_cand, const int *k_vals, int num_k_vals, int backward,
