@@ -219,7 +219,8 @@ __device__ __forceinline__ float below(float x) { return x > 0.0f ? __int_as_flo
 // the stage (kSC columns each).  Items go in column order with the reference
 // rule (after every element <= d, entry below the k-th once the list is
 // full); every lane recomputes each item's exact distance from shared
-// memory, and the list being filled sits in registers, lane j holding entry j.
+// memory, and the list being filled sits in registers, lane j holding entry j
+// (entries 2j and 2j+1 for k_max > 32).
 // Returns a mask of the warp's rows (bit p / kCW) whose thresholds may have
 // changed.
 template <bool BWD, int KL>
@@ -235,77 +236,102 @@ __device__ __forceinline__ unsigned insert_chunk(unsigned pm, const float *D_s, 
         any &= ~(3u << (2 * p));
         float *L = myL + p * KL;
         int *LI = myI + p * KL;
-        // lane j holds entry j (and, for k_max > 32, entry j + 32)
-        float L0 = lane < K ? L[lane] : INFINITY;
-        int I0 = lane < K ? LI[lane] : 0;
-        float L1 = INFINITY;
-        int I1 = 0;
-        if constexpr (LONG) {
-            L1 = lane + 32 < K ? L[lane + 32] : INFINITY;
-            I1 = lane + 32 < K ? LI[lane + 32] : 0;
-        }
         float th = myT[p];
         const float xv = myX[p];
         const float *xrow = X_s + (p % kCW) * kSC + q0;
         const float *dr = D_s + (p / kCW) * kSC + q0;
         const unsigned mine = (pm >> (2 * p)) & 3u;
         unsigned m = __ballot_sync(kFull, mine != 0u);
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const unsigned hb = __shfl_sync(kFull, mine, l);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (!((hb >> h) & 1u)) continue;
-                const int c = 2 * l + h;
-                const float s1 = sqdiff1(xv, xrow[c]);
-                const float d = BWD ? __fsub_rn(dr[c], s1) : __fadd_rn(dr[c], s1);
-                if (d <= th) {
-                    // d < FLT_MAX and, for a full list, d < k-th: the slot is < K
-                    int pos = __popc(__ballot_sync(kFull, lane < K && L0 <= d));
-                    const float up0 = __shfl_up_sync(kFull, L0, 1);
-                    const int upi0 = __shfl_up_sync(kFull, I0, 1);
-                    if constexpr (LONG) {
-                        pos += __popc(__ballot_sync(kFull, lane + 32 < K && L1 <= d));
-                        // entry 31 moves to entry 32 (lane 0 of the second half)
-                        float up1 = __shfl_up_sync(kFull, L1, 1);
-                        int upi1 = __shfl_up_sync(kFull, I1, 1);
-                        const float c31 = __shfl_sync(kFull, L0, 31);
-                        const int ci31 = __shfl_sync(kFull, I0, 31);
-                        if (lane == 0) {
-                            up1 = c31;
-                            upi1 = ci31;
-                        }
-                        if (lane + 32 == pos) {
-                            L1 = d;
-                            I1 = colbase + c;
-                        } else if (lane + 32 > pos) {
-                            L1 = up1;
-                            I1 = upi1;
-                        }
-                    }
-                    if (lane == pos) {
-                        L0 = d;
-                        I0 = colbase + c;
-                    } else if (lane > pos) {
-                        L0 = up0;
-                        I0 = upi0;
-                    }
-                    float kth;
-                    if constexpr (LONG) kth = K <= 32 ? __shfl_sync(kFull, L0, (K - 1) & 31) : __shfl_sync(kFull, L1, (K - 33) & 31);
-                    else kth = __shfl_sync(kFull, L0, K - 1);
-                    if (kth < FLT_MAX) th = BWD ? nextafterf(kth, -INFINITY) : below(kth);
+        if constexpr (LONG) {
+            // k_max > 32: lane j holds the adjacent entries 2j and 2j+1 (one
+            // 64-bit shared-memory access each for distances and columns), so
+            // an insertion shifts the list with one shuffle per array
+            const int e0 = 2 * lane;
+            float2 Lv = make_float2(INFINITY, INFINITY);
+            int2 Iv = make_int2(0, 0);
+            if (e0 < K) {
+                Lv = *reinterpret_cast<const float2 *>(L + e0);
+                Iv = *reinterpret_cast<const int2 *>(LI + e0);
+                if (e0 + 1 >= K) {
+                    Lv.y = INFINITY;
+                    Iv.y = 0;
                 }
             }
-        }
-        if (lane < K) {
-            L[lane] = L0;
-            LI[lane] = I0;
-        }
-        if constexpr (LONG) {
-            if (lane + 32 < K) {
-                L[lane + 32] = L1;
-                LI[lane + 32] = I1;
+            while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                const unsigned hb = __shfl_sync(kFull, mine, l);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (!((hb >> h) & 1u)) continue;
+                    const int c = 2 * l + h;
+                    const float s1 = sqdiff1(xv, xrow[c]);
+                    const float d = BWD ? __fsub_rn(dr[c], s1) : __fadd_rn(dr[c], s1);
+                    if (d <= th) {
+                        // d < FLT_MAX and, for a full list, d < k-th: the slot is < K
+                        const int pos = __popc(__ballot_sync(kFull, e0 < K && Lv.x <= d)) +
+                                        __popc(__ballot_sync(kFull, e0 + 1 < K && Lv.y <= d));
+                        const float pL = __shfl_up_sync(kFull, Lv.y, 1);  // entry 2j - 1
+                        const int pI = __shfl_up_sync(kFull, Iv.y, 1);
+                        // entry 2j + 1 first: it may take the old entry 2j
+                        if (e0 + 1 == pos) {
+                            Lv.y = d;
+                            Iv.y = colbase + c;
+                        } else if (e0 + 1 > pos) {
+                            Lv.y = Lv.x;
+                            Iv.y = Iv.x;
+                        }
+                        if (e0 == pos) {
+                            Lv.x = d;
+                            Iv.x = colbase + c;
+                        } else if (e0 > pos) {
+                            Lv.x = pL;
+                            Iv.x = pI;
+                        }
+                        const float kth = __shfl_sync(kFull, ((K - 1) & 1) ? Lv.y : Lv.x, (K - 1) >> 1);
+                        if (kth < FLT_MAX) th = BWD ? nextafterf(kth, -INFINITY) : below(kth);
+                    }
+                }
+            }
+            // with K odd, lane (K-1)/2 also writes slot K, which lies past the list and is never read
+            if (e0 < K) {
+                *reinterpret_cast<float2 *>(L + e0) = Lv;
+                *reinterpret_cast<int2 *>(LI + e0) = Iv;
+            }
+        } else {
+            // lane j holds entry j
+            float L0 = lane < K ? L[lane] : INFINITY;
+            int I0 = lane < K ? LI[lane] : 0;
+            while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                const unsigned hb = __shfl_sync(kFull, mine, l);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (!((hb >> h) & 1u)) continue;
+                    const int c = 2 * l + h;
+                    const float s1 = sqdiff1(xv, xrow[c]);
+                    const float d = BWD ? __fsub_rn(dr[c], s1) : __fadd_rn(dr[c], s1);
+                    if (d <= th) {
+                        // d < FLT_MAX and, for a full list, d < k-th: the slot is < K
+                        const int pos = __popc(__ballot_sync(kFull, lane < K && L0 <= d));
+                        const float up0 = __shfl_up_sync(kFull, L0, 1);
+                        const int upi0 = __shfl_up_sync(kFull, I0, 1);
+                        if (lane == pos) {
+                            L0 = d;
+                            I0 = colbase + c;
+                        } else if (lane > pos) {
+                            L0 = up0;
+                            I0 = upi0;
+                        }
+                        const float kth = __shfl_sync(kFull, L0, K - 1);
+                        if (kth < FLT_MAX) th = BWD ? nextafterf(kth, -INFINITY) : below(kth);
+                    }
+                }
+            }
+            if (lane < K) {
+                L[lane] = L0;
+                LI[lane] = I0;
             }
         }
         if (lane == 0) myT[p] = th;
