@@ -174,7 +174,8 @@ __global__ void __launch_bounds__(256) k_first_step(Bufs b, const float *sv, con
 // left, lanes 16-31 the next 16 on the right (all 32 lanes the open side once
 // the other is finished); columns whose D already exceeds
 // the k-th distance are skipped, and the few that pass are inserted into
-// a register-held list (lane j holds entry j, and j + 32 when k > 32) sorted
+// a register-held list (lane j holds entry j; k_second_step_long below keeps
+// k in (32, 64]) sorted
 // by (distance, index) -- columns arrive out of index order, and that order
 // is the reference's stable one.  D is recomputed from the sorted values (the
 // commit's rounding), not read from memory, and the candidates' values come
@@ -200,12 +201,10 @@ __global__ void __launch_bounds__(256) k_gather_sorted(Bufs b, const int *si, fl
     xs[(size_t)slot * b.ldc + j] = __ldg(b.XT + (size_t)c * b.ldc + __ldg(si + (size_t)w * b.ldc + j));
 }
 
-template <int KL>
 __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, const int *si, const float *xs,
                                                      int n_cand, unsigned long long *walked,
                                                      unsigned long long budget)
 {
-    constexpr bool LONG = KL > 32;
     constexpr unsigned kFull = 0xffffffffu;
     if (b.st->done) return;
     const int lane = threadIdx.x & 31;
@@ -222,9 +221,9 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
     const int *bi = si + (size_t)w * b.ldc;
     const float *xsc = xs + (size_t)slot * b.ldc;
 
-    // the list: entry e (e < cnt) at lane e (L0, I0) or lane e - 32 (L1, I1)
-    float L0 = INFINITY, L1 = INFINITY;
-    int I0 = 0x7fffffff, I1 = 0x7fffffff;
+    // the list: entry e (e < cnt) at lane e
+    float L0 = INFINITY;
+    int I0 = 0x7fffffff;
     int cnt = 0;
     float th = INFINITY;  // the k-th entry once the list is full
     int thi = 0x7fffffff;
@@ -290,27 +289,9 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
                 const int iv = __shfl_sync(kFull, i, l);
                 if (!(dv < th || (dv == th && iv < thi))) continue;  // the list tightened meanwhile
                 // position: entries ordered before (dv, iv)
-                int pos = __popc(__ballot_sync(kFull, lane < cnt && (L0 < dv || (L0 == dv && I0 < iv))));
+                const int pos = __popc(__ballot_sync(kFull, lane < cnt && (L0 < dv || (L0 == dv && I0 < iv))));
                 const float up0 = __shfl_up_sync(kFull, L0, 1);
                 const int upi0 = __shfl_up_sync(kFull, I0, 1);
-                if constexpr (LONG) {
-                    pos += __popc(__ballot_sync(kFull, lane + 32 < cnt && (L1 < dv || (L1 == dv && I1 < iv))));
-                    float up1 = __shfl_up_sync(kFull, L1, 1);
-                    int upi1 = __shfl_up_sync(kFull, I1, 1);
-                    const float c31 = __shfl_sync(kFull, L0, 31);
-                    const int ci31 = __shfl_sync(kFull, I0, 31);
-                    if (lane == 0) {
-                        up1 = c31;
-                        upi1 = ci31;
-                    }
-                    if (lane + 32 == pos) {
-                        L1 = dv;
-                        I1 = iv;
-                    } else if (lane + 32 > pos && lane + 32 < K) {
-                        L1 = up1;
-                        I1 = upi1;
-                    }
-                }
                 if (lane == pos) {
                     L0 = dv;
                     I0 = iv;
@@ -320,13 +301,8 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
                 }
                 if (cnt < K) ++cnt;
                 if (cnt == K) {
-                    if constexpr (LONG) {
-                        th = K <= 32 ? __shfl_sync(kFull, L0, (K - 1) & 31) : __shfl_sync(kFull, L1, (K - 33) & 31);
-                        thi = K <= 32 ? __shfl_sync(kFull, I0, (K - 1) & 31) : __shfl_sync(kFull, I1, (K - 33) & 31);
-                    } else {
-                        th = __shfl_sync(kFull, L0, K - 1);
-                        thi = __shfl_sync(kFull, I0, K - 1);
-                    }
+                    th = __shfl_sync(kFull, L0, K - 1);
+                    thi = __shfl_sync(kFull, I0, K - 1);
                 }
             }
             // a side is finished past its end or once its farthest D of this batch exceeds the k-th
@@ -342,27 +318,228 @@ __global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, co
         L0 = FLT_MAX;
         I0 = 0;
     }
-    if (lane + 32 >= cnt) {
-        L1 = FLT_MAX;
-        I1 = 0;
-    }
     if (b.nn_idx) {
         const size_t o = ((size_t)slot * b.n_rows + r) * K;
         if (lane < K) {
             b.nn_idx[o + lane] = I0;
             b.nn_dist[o + lane] = L0;
         }
-        if (LONG && lane + 32 < K) {
-            b.nn_idx[o + lane + 32] = I1;
-            b.nn_dist[o + lane + 32] = L1;
-        }
     }
     // labels summed in rank order (sequential FP32) by lane 0, as the scoring kernels
     const float y0 = lane < K ? __ldg(b.yc + I0) : 0.0f;
-    const float y1 = LONG && lane + 32 < K ? __ldg(b.yc + I1) : 0.0f;
     float acc = 0.0f;
     for (int e = 0; e < K; ++e) {
-        const float ye = e < 32 ? __shfl_sync(kFull, y0, e) : __shfl_sync(kFull, y1, e - 32);
+        const float ye = __shfl_sync(kFull, y0, e);
+        acc = __fadd_rn(acc, ye);
+        if (lane == 0)
+            for (int m = 0; m < b.nk; ++m) {
+                const int k = __ldg(b.kvals + m);
+                if (k == e + 1) b.pred[((size_t)slot * b.nk + m) * b.n_rows + r] = __fdiv_rn(acc, (float)k);
+            }
+    }
+}
+
+
+// Ascending bitonic sort of 64 keys over the warp, two per lane: lane l ends
+// with elements 2l and 2l+1.
+__device__ __forceinline__ void warp_sort64x2(unsigned long long (&v)[2], int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 2) {  // partner in lane ^ (j / 2), same slot
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const unsigned long long o = __shfl_xor_sync(0xffffffffu, v[h], j >> 1);
+                    const int i = 2 * lane + h;
+                    v[h] = (((i & j) == 0) == ((i & k) == 0)) ? min(v[h], o) : max(v[h], o);
+                }
+            } else {  // partner in the same lane
+                const bool up = ((2 * lane) & k) == 0;
+                const unsigned long long a = v[0], c = v[1];
+                v[0] = up ? min(a, c) : max(a, c);
+                v[1] = up ? max(a, c) : min(a, c);
+            }
+        }
+    }
+}
+
+// k_second_step_long: the walk of k_second_step for 32 < k <= 64.  The list
+// sits as adjacent pairs (lane j holds entries 2j and 2j+1), so an insertion
+// shifts it with one shuffle per array; and the first 64 columns (32 per side,
+// or 64 on the side still open) are read together and sorted into the list at
+// once, so with k finite distances among them the list is full -- and the
+// walk's sides can finish -- from the first batch on.
+__global__ void __launch_bounds__(256) k_second_step_long(Bufs b, const float *sv, const int *si, const float *xs,
+                                                          int n_cand, unsigned long long *walked,
+                                                          unsigned long long budget)
+{
+    constexpr unsigned kFull = 0xffffffffu;
+    if (b.st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int slot = blockIdx.y;
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= n_cand || r >= b.n_rows) return;  // warp-uniform
+    const int K = b.kmax;
+    const int n = b.n_cols;
+    const int w = b.st->winner;
+    const int c = b.cands[slot];
+    const float aw = b.XV[(size_t)w * b.ldr + r];
+    const float ac = b.XV[(size_t)c * b.ldr + r];
+    const float *bv = sv + (size_t)w * b.ldc;
+    const int *bi = si + (size_t)w * b.ldc;
+    const float *xsc = xs + (size_t)slot * b.ldc;
+    // the list: entries e0 = 2 * lane and e0 + 1 (valid below cnt)
+    const int e0 = 2 * lane;
+    float2 Lv = make_float2(INFINITY, INFINITY);
+    int2 Iv = make_int2(0x7fffffff, 0x7fffffff);
+    int cnt = 0;
+    float th = INFINITY;  // the k-th entry once the list is full
+    int thi = 0x7fffffff;
+    // non-finite x_r,w or x_r,c: no distance below FLT_MAX, the list stays padding
+    if (isfinite(aw) && isfinite(ac)) {
+        int lo = 0, hi = n;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (bv[mid] < aw) lo = mid + 1;
+            else hi = mid;
+        }
+        int ln = lo - 1, rn = lo;  // next unvisited position on each side
+        bool ldone = ln < 0, rdone = rn >= n;
+        // batch position q: the left side's (q+1)-th next column for q < nl, else the right side's
+        auto visit = [&](int q, int nl, float &D, float &d, int &i) {
+            const bool left = q < nl;
+            const int j = left ? ln - q : rn + (q - nl);
+            const bool in = left ? j >= 0 : (!rdone && j < n);
+            // the three loads are independent (and contiguous across the lanes)
+            const float vj = in ? bv[j] : 0.0f, xj = in ? xsc[j] : 0.0f;
+            const int ij = in ? bi[j] : 0x7fffffff;
+            D = in ? dist1(aw, vj) : INFINITY;
+            d = INFINITY;
+            i = 0x7fffffff;
+            if (in && D <= th) {  // d >= D: beyond the k-th distance nothing enters
+                i = ij;
+                const float t = __fsub_rn(ac, xj);
+                d = __fadd_rn(D, __fmul_rn(t, t));
+            }
+        };
+        if (!(ldone && rdone)) {
+            // first batch, 64 columns: their finite distances sorted by (distance, index)
+            // (distances are >= +0, so their bits order like the values), the first K kept
+            const int nl = ldone ? 0 : (rdone ? 64 : 32);
+            float Da, da, Db, db;
+            int ia, ib;
+            visit(lane, nl, Da, da, ia);
+            visit(lane + 32, nl, Db, db, ib);
+            unsigned long long kk[2] = {
+                da < FLT_MAX ? ((unsigned long long)__float_as_uint(da) << 32) | (unsigned)ia : ~0ull,
+                db < FLT_MAX ? ((unsigned long long)__float_as_uint(db) << 32) | (unsigned)ib : ~0ull};
+            cnt = min(__popc(__ballot_sync(kFull, da < FLT_MAX)) + __popc(__ballot_sync(kFull, db < FLT_MAX)), K);
+            warp_sort64x2(kk, lane);
+            if (e0 < cnt) {
+                Lv.x = __uint_as_float((unsigned)(kk[0] >> 32));
+                Iv.x = (int)(unsigned)(kk[0] & 0xffffffffu);
+            }
+            if (e0 + 1 < cnt) {
+                Lv.y = __uint_as_float((unsigned)(kk[1] >> 32));
+                Iv.y = (int)(unsigned)(kk[1] & 0xffffffffu);
+            }
+            if (cnt == K) {
+                th = __shfl_sync(kFull, ((K - 1) & 1) ? Lv.y : Lv.x, (K - 1) >> 1);
+                thi = __shfl_sync(kFull, ((K - 1) & 1) ? Iv.y : Iv.x, (K - 1) >> 1);
+            }
+            // a side is finished past its end or once its farthest D of the batch exceeds the k-th
+            const int ql = nl > 0 ? nl - 1 : 0;
+            const float dl_far = __shfl_sync(kFull, ql < 32 ? Da : Db, ql & 31);
+            const float dr_far = __shfl_sync(kFull, Db, 31);
+            ln -= nl;
+            rn += 64 - nl;
+            ldone = ldone || ln < 0 || (nl > 0 && dl_far > th);
+            rdone = rdone || rn >= n || (nl < 64 && dr_far > th);
+        }
+        for (int it = 1; !(ldone && rdone); ++it) {
+            if ((it & 63) == 0) {  // account for the walk; leave when the budget is spent
+                int stop = 0;
+                if (lane == 0) {
+                    const unsigned long long tot = atomicAdd(walked, 64ull * 32ull) + 64ull * 32ull;
+                    if (tot > budget) atomicExch(&b.st->full_scan, 1);
+                    stop = tot > budget || *(volatile int *)&b.st->full_scan;
+                }
+                if (__shfl_sync(kFull, stop, 0)) return;
+            }
+            // 16 columns per side, or all 32 lanes on the side still open
+            const int nl = ldone ? 0 : (rdone ? 32 : 16);
+            float D, d;
+            int i;
+            visit(lane, nl, D, d, i);
+            unsigned m = __ballot_sync(kFull, d < FLT_MAX && (d < th || (d == th && i < thi)));
+            while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                const float dv = __shfl_sync(kFull, d, l);
+                const int iv = __shfl_sync(kFull, i, l);
+                if (!(dv < th || (dv == th && iv < thi))) continue;  // the list tightened meanwhile
+                // position: entries ordered before (dv, iv)
+                const int pos = __popc(__ballot_sync(kFull, e0 < cnt && (Lv.x < dv || (Lv.x == dv && Iv.x < iv)))) +
+                                __popc(__ballot_sync(kFull, e0 + 1 < cnt && (Lv.y < dv || (Lv.y == dv && Iv.y < iv))));
+                const float pL = __shfl_up_sync(kFull, Lv.y, 1);  // entry 2j - 1
+                const int pI = __shfl_up_sync(kFull, Iv.y, 1);
+                // entry 2j + 1 first: it may take the old entry 2j
+                if (e0 + 1 == pos) {
+                    Lv.y = dv;
+                    Iv.y = iv;
+                } else if (e0 + 1 > pos && e0 + 1 < K) {
+                    Lv.y = Lv.x;
+                    Iv.y = Iv.x;
+                }
+                if (e0 == pos) {
+                    Lv.x = dv;
+                    Iv.x = iv;
+                } else if (e0 > pos && e0 < K) {
+                    Lv.x = pL;
+                    Iv.x = pI;
+                }
+                if (cnt < K) ++cnt;
+                if (cnt == K) {
+                    th = __shfl_sync(kFull, ((K - 1) & 1) ? Lv.y : Lv.x, (K - 1) >> 1);
+                    thi = __shfl_sync(kFull, ((K - 1) & 1) ? Iv.y : Iv.x, (K - 1) >> 1);
+                }
+            }
+            // a side is finished past its end or once its farthest D of this batch exceeds the k-th
+            const float dl_far = __shfl_sync(kFull, D, nl > 0 ? nl - 1 : 0), dr_far = __shfl_sync(kFull, D, 31);
+            ln -= nl;
+            rn += 32 - nl;
+            ldone = ldone || ln < 0 || (nl > 0 && dl_far > th);
+            rdone = rdone || rn >= n || (nl < 32 && dr_far > th);
+        }
+    }
+    // entries past cnt are padding (FLT_MAX, 0)
+    if (e0 >= cnt) {
+        Lv.x = FLT_MAX;
+        Iv.x = 0;
+    }
+    if (e0 + 1 >= cnt) {
+        Lv.y = FLT_MAX;
+        Iv.y = 0;
+    }
+    if (b.nn_idx) {
+        const size_t o = ((size_t)slot * b.n_rows + r) * K;
+        if (e0 < K) {
+            b.nn_idx[o + e0] = Iv.x;
+            b.nn_dist[o + e0] = Lv.x;
+        }
+        if (e0 + 1 < K) {
+            b.nn_idx[o + e0 + 1] = Iv.y;
+            b.nn_dist[o + e0 + 1] = Lv.y;
+        }
+    }
+    // labels summed in rank order (sequential FP32) by lane 0, as the scoring kernels
+    const float y0 = e0 < K ? __ldg(b.yc + Iv.x) : 0.0f;
+    const float y1 = e0 + 1 < K ? __ldg(b.yc + Iv.y) : 0.0f;
+    float acc = 0.0f;
+    for (int e = 0; e < K; ++e) {
+        const float ye = __shfl_sync(kFull, (e & 1) ? y1 : y0, e >> 1);
         acc = __fadd_rn(acc, ye);
         if (lane == 0)
             for (int m = 0; m < b.nk; ++m) {
@@ -404,8 +581,8 @@ cudaError_t launch_second_step(const Bufs &b, const float *sv, const int *si, fl
     k_gather_sorted<<<dim3((b.n_cols + 255) / 256, n_cand), 256, 0, s>>>(b, si, xs, n_cand);
     const unsigned long long budget = (unsigned long long)b.n_rows * (unsigned long long)n_cand * b.n_cols / 8;
     const dim3 grid((b.n_rows + 7) / 8, n_cand);  // a warp per (candidate, row)
-    if (b.kmax <= 32) k_second_step<32><<<grid, 256, 0, s>>>(b, sv, si, xs, n_cand, walked, budget);
-    else if (b.kmax <= 64) k_second_step<64><<<grid, 256, 0, s>>>(b, sv, si, xs, n_cand, walked, budget);
+    if (b.kmax <= 32) k_second_step<<<grid, 256, 0, s>>>(b, sv, si, xs, n_cand, walked, budget);
+    else if (b.kmax <= 64) k_second_step_long<<<grid, 256, 0, s>>>(b, sv, si, xs, n_cand, walked, budget);
     else return cudaErrorInvalidValue;  // k above 64 scans
     return cudaGetLastError();
 }
