@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(256) k_gather_sorted(Bufs b, const int *si, fl
     xs[(size_t)slot * b.ldc + j] = __ldg(b.XT + (size_t)c * b.ldc + __ldg(si + (size_t)w * b.ldc + j));
 }
 
-__global__ void __launch_bounds__(256) k_second_step(Bufs b, const float *sv, const int *si, const float *xs,
+__global__ void __launch_bounds__(256, 8) k_second_step(Bufs b, const float *sv, const int *si, const float *xs,
                                                      int n_cand, unsigned long long *walked,
                                                      unsigned long long budget)
 {
@@ -371,7 +371,7 @@ __device__ __forceinline__ void warp_sort64x2(unsigned long long (&v)[2], int la
 // or 64 on the side still open) are read together and sorted into the list at
 // once, so with k finite distances among them the list is full -- and the
 // walk's sides can finish -- from the first batch on.
-__global__ void __launch_bounds__(256) k_second_step_long(Bufs b, const float *sv, const int *si, const float *xs,
+__global__ void __launch_bounds__(256, 8) k_second_step_long(Bufs b, const float *sv, const int *si, const float *xs,
                                                           int n_cand, unsigned long long *walked,
                                                           unsigned long long budget)
 {
