@@ -52,6 +52,9 @@ WORKLOAD = "fwd-64k"
 # 544.2 + 8.3 MB for 8192 x 16384 pairs): the D stream read once plus the small
 # X, bound and label traffic.
 TRAFFIC_PER_PAIR = 552.44e6 / (8192 * 16384)
+# The same for the 64-slot lists (k in (32, 64]), from a seeded step with k = 50
+# on 15,000 x 30,000 pairs: 1845.4 + 29.9 MB.
+TRAFFIC_PER_PAIR_K64 = 1875.35e6 / (15000 * 30000)
 METRIC = "cand-evals/s (n_val*n_train*candidates per second), greedy forward selection"
 UNIT = "cand-evals/s"
 
@@ -529,11 +532,14 @@ def run_ours(args, world, rank, local):
                                         "arithmetic ops only",
                          "hbm_achieved_gbs": achieved_hbm, "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src,
                          "hbm_frac": achieved_hbm / hbm,
-                         "traffic": args.traffic if args.traffic is not None else TRAFFIC_PER_PAIR * n_val * n_train,
+                         "traffic": args.traffic if args.traffic is not None else
+                         (TRAFFIC_PER_PAIR_K64 if 32 < k <= 64 else TRAFFIC_PER_PAIR) * n_val * n_train,
                          "traffic_source": "command line" if args.traffic is not None else
-                         "ncu dram__bytes_read.sum + dram__bytes_write.sum of one seeded k_score_tma launch on "
-                         "the 16384 x 8192 case (552.4 MB, profiles/k_score_tma_small_ncu.md), scaled per "
-                         "(validation row, training row) pair"},
+                         ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one seeded k_score_tma launch on "
+                          + ("the k = 50, 30000 x 15000 case (1875.4 MB, profiles/k_score_tma_k50_small_ncu.md)"
+                             if 32 < k <= 64 else
+                             "the 16384 x 8192 case (552.4 MB, profiles/k_score_tma_small_ncu.md)")
+                          + ", scaled per (validation row, training row) pair")},
             "clocks": clocks,
             "result": {"ordering": [int(x) for x in res["ordering"][:steps]],
                        "errors": [float(x) for x in res["errors"][:steps]]}}
