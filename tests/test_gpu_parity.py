@@ -418,13 +418,14 @@ def _first_step_data(kind, rng):
 
 
 @pytest.mark.parametrize("kind", ["plain", "duplicates", "quantized", "nonfinite", "few_rows"])
-@pytest.mark.parametrize("kv", [[10], [3, 45]])
+@pytest.mark.parametrize("kv", [[10], [3, 45], [64, 1], [33]])
 def test_sorted_first_steps_equal_scan(kind, kv):
     """The first two forward steps from sorted feature columns (a window
     around each row's value, then a walk of the first winner's values) against
     the scan of every column: identical neighbour lists of every candidate and
     row at both steps, and identical selections (quantized values exercise the
-    hand-back to the scan)."""
+    hand-back to the scan).  k above 32 takes the walk whose first 64 columns
+    fill the list at once (k = 64 exactly, k = 33 and 45 odd)."""
     rng = np.random.default_rng(101)
     Xt, yt, Xv, yv = _first_step_data(kind, rng)
     out = {}
