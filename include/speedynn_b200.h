@@ -268,6 +268,13 @@ SNN_API int snn_batch_create(const snn_desc *descs, int n, unsigned long long ma
 SNN_API int snn_batch_load(snn_batch *b, int i, const float *X_train, const float *y_train, const float *X_val,
                            const float *y_val);
 
+/* Problem i's losses and model, as snn_set_model on a handle (loss ids 0..8,
+ * the first decides; model_type 0 regression, 1 classification).  Call
+ * before snn_batch_run; default {RMSE}, regression.  Counterpart:
+ * train_*_selection's loss_functions and model_type
+ * (speedynn/lib/nearest_neighbors_feature_selection.h:59-80). */
+SNN_API int snn_batch_set_model(snn_batch *b, int i, const int *loss_ids, int n_losses, int model_type);
+
 /* Run every problem's whole selection; blocks until all are done.  A failing
  * problem keeps its status for snn_batch_get_results; device or argument
  * errors stop the batch with a negative status. */
@@ -276,6 +283,10 @@ SNN_API int snn_batch_run(snn_batch *b);
 /* Problem i's results, as snn_get_results; returns that problem's status. */
 SNN_API int snn_batch_get_results(snn_batch *b, int i, int *ordering, int *mask, float *errors, double *errors64,
                                   int *step_best_k, int *best_k, int *num_final);
+
+/* Problem i's errors of every loss for each step's winner, as
+ * snn_get_errors_all ([loss][step slot], n >= n_losses * p). */
+SNN_API int snn_batch_get_errors_all(snn_batch *b, int i, float *errors, int n);
 
 /* Device time of the last snn_batch_run's selections, and the number of
  * waves.  Each problem's selection is issued on its stream as soon as the

@@ -87,6 +87,8 @@ def lib():
             "snn_batch_create": (ctypes.c_int, [ctypes.POINTER(SnnDesc), ctypes.c_int, ctypes.c_ulonglong,
                                                 ctypes.POINTER(vp)]),
             "snn_batch_load": (ctypes.c_int, [vp, ctypes.c_int, _f32p, _f32p, _f32p, _f32p]),
+            "snn_batch_set_model": (ctypes.c_int, [vp, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int]),
+            "snn_batch_get_errors_all": (ctypes.c_int, [vp, ctypes.c_int, _f32p, ctypes.c_int]),
             "snn_batch_run": (ctypes.c_int, [vp]),
             "snn_batch_get_results": (ctypes.c_int, [vp, ctypes.c_int, _i32p, _i32p, _f32p, _f64p, _i32p, _i32p,
                                                      _i32p]),

@@ -2,7 +2,9 @@
 
 Each problem is a dict with the Selector keywords: ``Xtrain``, ``ytrain``,
 optional ``Xval``/``yval`` (holdout; CV mode without them), ``k_vals``,
-``num_features``, ``method``, ``k_fold``, ``auto_feature``, ``device``.
+``num_features``, ``method``, ``k_fold``, ``auto_feature``, ``device``,
+``loss_functions`` (reference loss ids, the first decides) and
+``model_type`` (0 regression, 1 classification).
 Problems run on their own CUDA streams so that small ones overlap on the
 GPU; the library groups them into waves that fit the device memory.  Each
 problem's results equal a Selector run of that problem alone.
@@ -25,6 +27,7 @@ class Batch:
         self._keep = []
         descs = (_lib.SnnDesc * len(problems))()
         self.p = []
+        self.models = []  # (loss ids, model type) per problem
         for i, pr in enumerate(problems):
             Xt = _f32(pr["Xtrain"])
             yt = _f32(pr["ytrain"]).reshape(-1)
@@ -47,12 +50,17 @@ class Batch:
             d.k_fold = int(pr.get("k_fold", 10))
             d.auto_feature = int(bool(pr.get("auto_feature", False)))
             d.device = int(pr.get("device", 0))
+            lf = np.ascontiguousarray(pr.get("loss_functions", (0,)), dtype=np.int32).reshape(-1)
             self._keep.append((Xt, yt, Xv, yv, kv))
             self.p.append(Xt.shape[1])
+            self.models.append((lf, int(pr.get("model_type", 0))))
         h = ctypes.c_void_p()
         check(L.snn_batch_create(descs, len(problems), int(max_device_bytes), ctypes.byref(h)))
         self._h = h
         try:
+            for i, (lf, mt) in enumerate(self.models):
+                if list(lf) != [0] or mt != 0:
+                    check(L.snn_batch_set_model(h, i, ptr(lf, _i32p), lf.size, mt))
             for i, (Xt, yt, Xv, yv, _) in enumerate(self._keep):
                 check(L.snn_batch_load(h, i, ptr(Xt, _f32p), ptr(yt, _f32p), None if Xv is None else ptr(Xv, _f32p),
                                        None if yv is None else ptr(yv, _f32p)))
@@ -75,6 +83,10 @@ class Batch:
                                                ptr(out["step_best_k"], _i32p), ctypes.byref(bk), ctypes.byref(nf)))
         out["best_k"] = bk.value
         out["num_final"] = nf.value
+        nl = self.models[i][0].size
+        ea = np.zeros(nl * p, np.float32)
+        check(_lib.lib().snn_batch_get_errors_all(self._h, i, ptr(ea, _f32p), ea.size))
+        out["errors_all"] = ea.reshape(nl, p)  # [loss][step slot], as Selector.results
         return out
 
     def timing(self):

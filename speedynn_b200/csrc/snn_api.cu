@@ -747,9 +747,11 @@ SNN_API int snn_set_model(snn_handle *h, const int *loss_ids, int n_losses, int 
     if (model_type != 0 && model_type != 1) return fail(SNN_ERR_ARG, "model_type %d is not 0 or 1", model_type);
     SNN_CUDA(cudaSetDevice(h->device));
     SNN_CUDA(cudaStreamSynchronize(h->stream));
-    cudaFree(h->d_loss_ids);
-    cudaFree(h->lossval);
-    cudaFree(h->err_all);
+    if (!h->arena) {  // an arena's sub-allocations are freed with the arena
+        cudaFree(h->d_loss_ids);
+        cudaFree(h->lossval);
+        cudaFree(h->err_all);
+    }
     h->d_loss_ids = nullptr;
     h->lossval = h->err_all = nullptr;
     h->loss_ids.assign(loss_ids, loss_ids + n_losses);
@@ -1016,8 +1018,10 @@ struct snn_batch {
         std::vector<int> kvals;
         const float *Xt = nullptr, *yt = nullptr, *Xv = nullptr, *yv = nullptr;
         int status = SNN_ERR_STATE;  // until run
+        std::vector<int> loss_ids{0};  // snn_batch_set_model: losses (the first decides) and model type
+        int model = 0;
         std::vector<int> ordering, mask, stepk;
-        std::vector<float> err;
+        std::vector<float> err, err_all;
         std::vector<double> err64;
         int best_k = 0, num_final = 0;
     };
@@ -1028,6 +1032,20 @@ struct snn_batch {
 };
 
 namespace {
+
+// Device bytes snn_set_model adds to a batch problem's handle: the loss ids,
+// every (loss, candidate, k) value and the winners' losses when a loss list
+// other than {RMSE} is set; the neighbour lists for classification.  Each
+// buffer may take up to 256 bytes more for its alignment in the arena.
+size_t model_bytes(const snn_batch::Problem &P, int kmax)
+{
+    const size_t nl = P.loss_ids.size(), p = (size_t)P.desc.p, nk = (size_t)P.desc.num_k_vals;
+    const size_t n_rows = P.desc.n_val > 0 ? (size_t)P.desc.n_val : (size_t)P.desc.n_train;
+    size_t f = 0;
+    if (P.loss_ids != std::vector<int>{0}) f += nl + nl * p * nk + nl * p;
+    if (P.model == 1) f += 2 * p * n_rows * (size_t)kmax;
+    return sizeof(float) * f + 5 * 256;
+}
 
 // Issue a loaded batch problem's whole selection on its own stream, between
 // its total_ev events (snn_load has just reset it), without waiting.
@@ -1064,6 +1082,8 @@ int finish_wave(snn_batch *B, std::vector<snn_handle *> &hs, int i0)
         if (int rc = snn_get_results(h, P.ordering.data(), P.mask.data(), P.err.data(), P.err64.data(), P.stepk.data(),
                                      &P.best_k, &P.num_final))
             P.status = rc;
+        P.err_all.assign(P.loss_ids.size() * p, 0.0f);
+        if (int rc = snn_get_errors_all(h, P.err_all.data(), (int)P.err_all.size())) P.status = rc;
         float a = 0.0f, b = 0.0f;  // relative to the first problem's start event
         SNN_CUDA(cudaEventElapsedTime(&a, hs[0]->total_ev.a, h->total_ev.a));
         SNN_CUDA(cudaEventElapsedTime(&b, hs[0]->total_ev.a, h->total_ev.b));
@@ -1127,6 +1147,20 @@ SNN_API int snn_batch_load(snn_batch *B, int i, const float *X_train, const floa
     return SNN_OK;
 }
 
+SNN_API int snn_batch_set_model(snn_batch *B, int i, const int *loss_ids, int n_losses, int model_type)
+{
+    g_err.clear();
+    if (!B || i < 0 || i >= (int)B->prob.size()) return fail(SNN_ERR_ARG, "snn_batch_set_model: no problem %d", i);
+    if (!loss_ids || n_losses <= 0) return fail(SNN_ERR_ARG, "at least one loss id is required");
+    for (int l = 0; l < n_losses; ++l)
+        if (loss_ids[l] < 0 || loss_ids[l] > 8) return fail(SNN_ERR_ARG, "loss id %d is not one of 0..8", loss_ids[l]);
+    if (model_type != 0 && model_type != 1) return fail(SNN_ERR_ARG, "model_type %d is not 0 or 1", model_type);
+    snn_batch::Problem &P = B->prob[i];
+    P.loss_ids.assign(loss_ids, loss_ids + n_losses);
+    P.model = model_type;
+    return SNN_OK;
+}
+
 SNN_API int snn_batch_run(snn_batch *B)
 {
     g_err.clear();
@@ -1154,7 +1188,7 @@ SNN_API int snn_batch_run(snn_batch *B)
         // (a wave always admits its first problem, whatever the budget)
         int kmax0 = 0;
         validate_desc(&B->prob[i].desc, &kmax0);
-        const size_t cap = std::max(budget, handle_bytes(&B->prob[i].desc, kmax0));
+        const size_t cap = std::max(budget, handle_bytes(&B->prob[i].desc, kmax0) + model_bytes(B->prob[i], kmax0));
         Arena arena;
         void *abase = nullptr;
         if (cudaMalloc(&abase, cap) == cudaSuccess) {
@@ -1170,12 +1204,14 @@ SNN_API int snn_batch_run(snn_batch *B)
         while (i < n && B->prob[i].desc.device == dev) {
             int kmax = 0;
             validate_desc(&B->prob[i].desc, &kmax);
-            const size_t need = handle_bytes(&B->prob[i].desc, kmax);
+            const snn_batch::Problem &P = B->prob[i];
+            const size_t need = handle_bytes(&P.desc, kmax) + model_bytes(P, kmax);
             if (!hs.empty() && used + need > budget) break;
             snn_handle *h = nullptr;
-            const snn_batch::Problem &P = B->prob[i];
             t_arena = arena.base ? &arena : nullptr;
             rc = snn_create(&P.desc, &h);
+            if (rc == SNN_OK && (P.loss_ids != std::vector<int>{0} || P.model != 0))
+                rc = snn_set_model(h, P.loss_ids.data(), (int)P.loss_ids.size(), P.model);
             if (rc == SNN_OK) {
                 h->step_events = false;  // only the selection's total events are read (finish_wave)
                 rc = load_impl(h, P.Xt, P.yt, P.Xv, P.yv, false, false);
@@ -1218,6 +1254,19 @@ SNN_API int snn_batch_get_results(snn_batch *B, int i, int *ordering, int *mask,
     if (step_best_k) memcpy(step_best_k, P.stepk.data(), sizeof(int) * p);
     if (best_k) *best_k = P.best_k;
     if (num_final) *num_final = P.num_final;
+    if (P.status) return fail(P.status, "problem %d ended with status %d", i, P.status);
+    return SNN_OK;
+}
+
+SNN_API int snn_batch_get_errors_all(snn_batch *B, int i, float *errors, int n)
+{
+    g_err.clear();
+    if (!B || i < 0 || i >= (int)B->prob.size()) return fail(SNN_ERR_ARG, "snn_batch_get_errors_all: no problem %d", i);
+    if (!errors) return fail(SNN_ERR_ARG, "null output");
+    const snn_batch::Problem &P = B->prob[i];
+    if (P.status == SNN_ERR_STATE && P.err_all.empty()) return fail(SNN_ERR_STATE, "problem %d has not run", i);
+    if (n < (int)P.err_all.size()) return fail(SNN_ERR_ARG, "errors needs %zu entries (losses x p)", P.err_all.size());
+    memcpy(errors, P.err_all.data(), sizeof(float) * P.err_all.size());
     if (P.status) return fail(P.status, "problem %d ended with status %d", i, P.status);
     return SNN_OK;
 }

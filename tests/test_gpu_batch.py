@@ -66,3 +66,41 @@ def test_many_concurrent_problems_match_single_runs():
         w = _alone(pr)
         for k in KEYS:
             np.testing.assert_array_equal(np.asarray(g[k]), np.asarray(w[k]), err_msg=f"problem {i}: {k}")
+
+
+def _model_problems():
+    """Problems with loss lists and the classification model: (n_train, n_val,
+    p, k values, features, method, loss ids, model type)."""
+    shapes = [(1400, 600, 11, [5, 1], 4, "forward", (4, 0), 1),   # classification, zero-one loss decides
+              (1000, 0, 10, [3, 9], 3, "backward", (0,), 1),      # classification, CV mode
+              (1200, 500, 12, [7], 5, "forward", (2, 0, 5), 0),   # MAD decides, RMSE and std kept
+              (800, 400, 9, [4, 20], 6, "backward", (1, 8), 0)]   # normalised RMSE decides
+    probs = []
+    for i, (nt, nv, p, kv, nf, method, lf, mt) in enumerate(shapes):
+        s = datagen.generate(nt, max(nv, 32), p, n_mag=5, seed=700 + i)
+        yt, yv = s.ytrain, s.yval
+        if mt == 1:  # class labels
+            yt = np.floor(3.0 * yt).astype(np.float32)
+            yv = np.floor(3.0 * yv).astype(np.float32)
+        pr = dict(Xtrain=s.Xtrain, ytrain=yt, k_vals=kv, num_features=nf, method=method, k_fold=4,
+                  loss_functions=lf, model_type=mt)
+        if nv:
+            pr.update(Xval=s.Xval, yval=yv)
+        probs.append(pr)
+    return probs
+
+
+@pytest.mark.parametrize("max_bytes", [0, 1])
+def test_batch_losses_and_classification_match_single_runs(max_bytes):
+    """snn_batch_set_model: each problem's selection, FP32 and FP64 errors and
+    the errors of every loss equal a Selector run with the same losses and
+    model, in one wave and in one wave per problem (the arena then holds
+    exactly one problem's buffers, the loss and neighbour arrays included)."""
+    probs = _model_problems()
+    want = [_alone(pr) for pr in probs]
+    with Batch(probs, max_device_bytes=max_bytes) as b:
+        got = b.run()
+    for w, g in zip(want, got):
+        for k in KEYS:
+            np.testing.assert_array_equal(np.asarray(g[k]), np.asarray(w[k]))
+        np.testing.assert_array_equal(g["errors_all"], w["errors_all"])
