@@ -137,3 +137,33 @@ def test_batch_rejects_bad_descriptors_without_a_gpu():
     assert "problem 1" in str(e.value)
     L = _lib.lib()
     assert L.snn_batch_create(None, 0, 0, None) == _lib.SNN_ERR_ARG
+
+
+def test_batch_model_arguments_are_checked_without_a_gpu():
+    """snn_batch_set_model checks the problem index, loss ids and model type
+    before anything runs; snn_batch_get_errors_all refuses a problem that has
+    not run.  None of it touches a device."""
+    import numpy as np
+    from speedynn_b200 import _lib
+    from speedynn_b200._lib import _f32p, _i32p, ptr
+    L = _lib.lib()
+    kv = np.array([3], np.int32)
+    d = (_lib.SnnDesc * 1)()
+    d[0].n_train, d[0].n_val, d[0].p = 50, 0, 4
+    d[0].k_vals, d[0].num_k_vals = ptr(kv, _i32p), 1
+    d[0].num_features, d[0].k_fold = 2, 5
+    h = ctypes.c_void_p()
+    assert L.snn_batch_create(d, 1, 0, ctypes.byref(h)) == _lib.SNN_OK
+    try:
+        ok = np.array([4, 0], np.int32)
+        assert L.snn_batch_set_model(h, 0, ptr(ok, _i32p), 2, 1) == _lib.SNN_OK
+        assert L.snn_batch_set_model(h, 1, ptr(ok, _i32p), 2, 0) == _lib.SNN_ERR_ARG  # no problem 1
+        bad = np.array([0, 9], np.int32)
+        assert L.snn_batch_set_model(h, 0, ptr(bad, _i32p), 2, 0) == _lib.SNN_ERR_ARG
+        assert b"loss id 9" in L.snn_last_error()
+        assert L.snn_batch_set_model(h, 0, ptr(ok, _i32p), 2, 2) == _lib.SNN_ERR_ARG
+        assert L.snn_batch_set_model(h, 0, None, 0, 0) == _lib.SNN_ERR_ARG
+        out = np.zeros(8, np.float32)
+        assert L.snn_batch_get_errors_all(h, 0, ptr(out, _f32p), out.size) == _lib.SNN_ERR_STATE
+    finally:
+        L.snn_batch_destroy(h)
